@@ -1,0 +1,57 @@
+"""Build oracle samplers from structure descriptor dicts (test infrastructure).
+
+The descriptor format is plain data (see the package's ``structures``
+module); this adapter only evaluates it with the oracle's samplers."""
+from __future__ import annotations
+
+import numpy as np
+
+from . import varrcwa_oracle as O
+
+
+def _pwl(zs, vals, z):
+    zs = np.asarray(zs, dtype=np.float64)
+    vals = np.asarray(vals, dtype=np.float64)
+    if z <= zs[0]:
+        return float(vals[0])
+    if z >= zs[-1]:
+        return float(vals[-1])
+    k = int(np.searchsorted(zs, z, side="right")) - 1
+    t = (z - zs[k]) / (zs[k + 1] - zs[k])
+    return float((1.0 - t) * vals[k] + t * vals[k + 1])
+
+
+def _pillar_raster(d, z):
+    npx, npy, Lx, Ly = d["npx"], d["npy"], d["Lx"], d["Ly"]
+    xc = (np.arange(npx) + 0.5) * (Lx / npx) - 0.5 * Lx
+    yc = (np.arange(npy) + 0.5) * (Ly / npy) - 0.5 * Ly
+    t = 0.0 if d["z1"] == d["z0"] else (z - d["z0"]) / (d["z1"] - d["z0"])
+    r = d["r0"] + (d["r1"] - d["r0"]) * t
+    inside = (xc[None, :] ** 2 + yc[:, None] ** 2) <= r * r
+    return np.where(inside, d["eps_in"], d["eps_out"]).astype(np.complex128)
+
+
+def make_sampler(d):
+    kind = d["kind"]
+    if kind == "grid":
+        s = O.VarLayerSampler(d["lam"], d["nx"], d["ny"], d["x"], d["y"], d["eps"],
+                              enable_pml=d["pml"])
+        for (i, zs, vals) in d.get("xrules", []):
+            s.add_x_rule(i, lambda z, zs=zs, vals=vals: _pwl(zs, vals, z))
+        for (j, zs, vals) in d.get("yrules", []):
+            s.add_y_rule(j, lambda z, zs=zs, vals=vals: _pwl(zs, vals, z))
+        return s
+    if kind == "pillar":
+        return O.RasterSampler(d["lam"], d["nx"], d["ny"], d["Lx"], d["Ly"],
+                               lambda z: _pillar_raster(d, z), enable_pml=d["pml"])
+    if kind == "pixels":
+        eps = np.asarray(d["eps"], dtype=np.complex128)
+        return O.RasterSampler(d["lam"], d["nx"], d["ny"], d["Lx"], d["Ly"],
+                               lambda z: eps, enable_pml=d["pml"])
+    raise ValueError(kind)
+
+
+def end_bases(d, sampler):
+    e0 = None if d.get("end0") is None else O.homogeneous_basis(sampler, d["end0"])
+    e1 = None if d.get("end1") is None else O.homogeneous_basis(sampler, d["end1"])
+    return e0, e1
