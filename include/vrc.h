@@ -1,0 +1,196 @@
+/*
+ * vrc.h -- C-ABI of the B200-native varRCWA hot path.
+ *
+ * Plain C types only (pointers, sizes, structs of scalars).  Every matrix is
+ * complex128, column-major with leading dimension n (the layout of
+ * Eigen::MatrixXcs and of the reference's cuDoubleComplex buffers), where
+ * n = 2*nx*ny (src/core/LayerSampler.h:44).  All buffers passed to these
+ * entry points are HOST memory unless stated otherwise.
+ *
+ * Each entry point returns a status code (vrc_status_code); on error
+ * vrc_last_error() describes it.  A context is bound to one CUDA device and
+ * is not thread-safe (the reference integrators are not either).
+ *
+ * The reference has no C-ABI; each function below lists the reference
+ * interface it replaces.
+ */
+#ifndef VRC_H_
+#define VRC_H_
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+  double re, im;
+} vrc_complex;
+
+typedef struct vrc_context vrc_context;
+
+enum vrc_status_code {
+  VRC_OK = 0,
+  VRC_EINVAL = 1,     /* invalid argument */
+  VRC_ECUDA = 2,      /* CUDA runtime error */
+  VRC_ENOMEM = 3,     /* device memory exhausted */
+  VRC_ESINGULAR = 4,  /* singular pivot in an LU / inverse */
+  VRC_ENOCONV = 5,    /* eigensolver did not converge within its iteration cap */
+  VRC_ENONFINITE = 6, /* non-finite value in a segment error estimate */
+  VRC_ETIMEOUT = 7,   /* reserved: bounded wait expired */
+  VRC_EDEPTH = 8,     /* adaptive recursion hit max_depth before the tolerance */
+  VRC_ENODEV = 9      /* no CUDA device / extension not usable */
+};
+
+enum vrc_geometry_kind {
+  VRC_GEOM_GRID = 0,   /* tensor grid, fixed eps table, moving coordinates */
+  VRC_GEOM_PILLAR = 1, /* uniform raster of a circular pillar, linear radius */
+  VRC_GEOM_PIXELS = 2  /* fixed uniform pixel raster (z-invariant) */
+};
+
+/* Piecewise-linear z-rule for one coordinate (clamped outside [zs0, zsN]).
+ * Replaces VarLayerSampler::addXRule/addYRule with a tabulated rule
+ * (src/core/VarLayerSampler.cpp:42-50). */
+typedef struct {
+  int index;
+  int nknots;
+  const double* zs;
+  const double* vals;
+} vrc_rule;
+
+/* Optional host callback evaluating arbitrary coordinate rules: called with
+ * the z of each sample and the coordinate arrays (already holding the base
+ * coordinates and the tabulated rules) to modify in place.  This is how a
+ * std::function rule of the reference reaches the engine. */
+typedef void (*vrc_geometry_fn)(void* user, double z, double* x, double* y);
+
+/* One structure.  Replaces VarLayerSampler(lambda, nx, ny, x, y, eps,
+ * enablePML) (src/core/VarLayerSampler.h:20-28) plus the z-range given to
+ * the integrators' constructors (src/core/RedhefferIntegrator.h:34-35). */
+typedef struct {
+  int kind;          /* vrc_geometry_kind */
+  int nx, ny;        /* harmonics per axis, odd; n = 2*nx*ny <= 1024 */
+  int pml;           /* 0: periodic, 1: PML on both lateral boundaries */
+  double lambda;     /* wavelength (same length unit as the geometry) */
+  double z0, z1;     /* integration range */
+  /* VRC_GEOM_GRID / VRC_GEOM_PIXELS */
+  int ncx, ncy;              /* number of x / y coordinates */
+  const double* x;           /* ncx */
+  const double* y;           /* ncy */
+  const vrc_complex* eps;    /* (ncy-1)*(ncx-1), row-major: rows are y strips */
+  int n_xrules;
+  const vrc_rule* xrules;
+  int n_yrules;
+  const vrc_rule* yrules;
+  vrc_geometry_fn geometry_fn; /* may be NULL */
+  void* geometry_user;
+  /* VRC_GEOM_PILLAR */
+  double Lx, Ly;
+  int npx, npy;
+  vrc_complex eps_in, eps_out;
+  double r0, r1; /* radius at z0 and at z1 */
+  /* homogeneous half-spaces joined at z0 / z1 (else the structure's own
+   * eigen-bases there, as the reference integrators do) */
+  int has_end0, has_end1;
+  vrc_complex eps_end0, eps_end1;
+} vrc_cell;
+
+/* Outputs of one integration.  Matrix pointers may be NULL (not copied). */
+typedef struct {
+  vrc_complex *Tdd, *Tuu, *Rud, *Rdu; /* n*n each */
+  vrc_complex *W0, *V0, *gam0;        /* basis at z0 (n*n, n*n, n) */
+  vrc_complex *W1, *V1, *gam1;        /* basis at z1 */
+  int status;                         /* per-cell vrc_status_code */
+  int n;                              /* matrix dimension */
+  int N;                              /* accepted segments / slices (N()) */
+  int n_eig;                          /* eigen-decompositions (nEigVal()) */
+  int n_samples;                      /* P,Q samples assembled */
+  int n_nodes;                        /* segments evaluated (accepted + rejected) */
+} vrc_result;
+
+/* Timing of the last integrator call (CUDA events on the engine stream). */
+typedef struct {
+  double device_ms;   /* first kernel to last kernel of the call */
+  long long launches; /* kernel launches issued by the call */
+} vrc_timing;
+
+/* ---- context ------------------------------------------------------------ */
+int vrc_create(int device, vrc_context** ctx);
+void vrc_destroy(vrc_context* ctx);
+const char* vrc_last_error(const vrc_context* ctx);
+const char* vrc_status_string(int status);
+int vrc_get_timing(const vrc_context* ctx, vrc_timing* t);
+
+/* ---- A1-A6: P,Q of the wave equation at given z (one structure) ---------
+ * Replaces LayerSampler::sample / sampleOnGPU (src/core/LayerSampler.h:49-55,
+ * src/core/VarLayerSampler.cpp:52-69, src/gpu/VarLayerSamplerGPU.cpp:130-214)
+ * over Layer::waveEqnCoeff (src/rcwa/Layer.cpp:36-171).
+ * P, Q: nz blocks of n*n. */
+int vrc_sample_pq(vrc_context* ctx, const vrc_cell* cell, int nz, const double* z, vrc_complex* P,
+                  vrc_complex* Q);
+
+/* ---- A7: eigen step -------------------------------------------------------
+ * Replaces WaveEquationSolver::solve (src/rcwa/WaveEquationSolver.cpp:24-37):
+ * W = eigenvectors of P*Q (unit 2-norm, largest component real),
+ * gam = sqrt(eig) on the reference branch, V = Q W diag(1/gam). */
+int vrc_wave_solve(vrc_context* ctx, int batch, int n, const vrc_complex* P, const vrc_complex* Q,
+                   vrc_complex* W, vrc_complex* V, vrc_complex* gam);
+/* Plain eigen-decomposition of batch n*n matrices A (replaces
+ * MKLEigenSolver::compute / LAPACKE_zgeev, src/rcwa/MKLEigenSolver.hpp:25-74). */
+int vrc_eig(vrc_context* ctx, int batch, int n, const vrc_complex* A, vrc_complex* W, vrc_complex* lam);
+
+/* ---- A8-A11: adaptive varRCWA ---------------------------------------------
+ * Replaces RedhefferIntegrator(z0, z1, sampler).compute(p, maxN, pe)
+ * (src/core/RedhefferIntegrator.h:34-50, RedhefferIntegrator.cpp:174-314)
+ * and RedhefferIntegratorGPU::compute_recursive
+ * (src/gpu/RedhefferIntegratorGPU.h:103).  `p` and `maxN` are unused by the
+ * reference and omitted; max_depth bounds the trisection depth. */
+int vrc_redheffer(vrc_context* ctx, int ncells, const vrc_cell* cells, double pe, int max_depth,
+                  vrc_result* results);
+/* varRCWA over explicit segment boundaries (cell c: ncuts[c] boundaries
+ * cuts[c][0]=z0 < ... < z1), each segment referenced at its midpoint.
+ * Replaces RedhefferIntegratorGPU::compute_direct(N) (uniform cuts,
+ * src/gpu/RedhefferIntegratorGPU.cpp:361-412) and replays a recorded tree. */
+int vrc_redheffer_segments(vrc_context* ctx, int ncells, const vrc_cell* cells, const int* ncuts,
+                           const double* const* cuts, vrc_result* results);
+/* Segmentation tree of cell `cell` of the last adaptive call: nodes in
+ * evaluation order (breadth-first).  Returns the node count (may exceed
+ * max_nodes; arrays hold the first max_nodes). */
+int vrc_get_tree(vrc_context* ctx, int cell, int max_nodes, double* a, double* b, double* err, int* accepted);
+
+/* ---- A12: plain RCWA --------------------------------------------------------
+ * Replaces RCWAIntegrator::compute(N) (src/core/RCWAIntegrator.cpp:20-87)
+ * and RCWAIntegratorGPU::compute(N) (src/gpu/RCWAIntegratorGPU.h:59). */
+int vrc_rcwa(vrc_context* ctx, int ncells, const vrc_cell* cells, int N, vrc_result* results);
+
+/* ---- A13: differential method ------------------------------------------------
+ * Replaces DifferentialIntegrator::compute(N)
+ * (src/core/DifferentialIntegrator.cpp:21-134). */
+int vrc_differential(vrc_context* ctx, int ncells, const vrc_cell* cells, int N, vrc_result* results);
+
+/* ---- A14: per-order power -----------------------------------------------------
+ * Integrate (method 0: adaptive varRCWA with pe/max_depth, 1: RCWA with
+ * N = nslices, 2: differential with N) and return per-order reflected /
+ * transmitted power for unit plane waves at normal incidence, polarisation
+ * (px,py) = (1,0) then (0,1): R and T hold ncells * 2 * (nx*ny) doubles.
+ * side 0: incidence from the z0 medium (Rdu, Tuu); 1: from z1 (Rud, Tdd, the
+ * reference's choice).  flux_norm 1 normalises T by the incident medium (so
+ * R+T = 1 when lossless); 0 divides by sqrt(eps_out) as the reference does.
+ * Replaces RCWASolver::scatterPlaneWave (src/rcwa/RCWASolver.cpp:1636-1733).
+ * Requires has_end0 = has_end1 = 1 and periodic boundaries; cells of one
+ * call may have different truncations (R/T offsets follow each cell's nx*ny
+ * in order). */
+int vrc_order_powers(vrc_context* ctx, int ncells, const vrc_cell* cells, int method, double pe, int max_depth,
+                     int nslices, int side, int flux_norm, double* R, double* T, int* status);
+
+/* ---- batched kernels (host buffers) --------------------------------------- */
+/* C[b] = A[b] * B[b]  (batch n*n complex GEMMs on FP64 tensor cores). */
+int vrc_zgemm(vrc_context* ctx, int batch, int n, const vrc_complex* A, const vrc_complex* B, vrc_complex* C);
+/* In-place inverse of batch n*n matrices; status[b] = VRC_ESINGULAR on a zero pivot. */
+int vrc_zinv(vrc_context* ctx, int batch, int n, vrc_complex* A, int* status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VRC_H_ */

@@ -1,0 +1,465 @@
+// extern "C" boundary (include/vrc.h) over the engine.
+#include "../../include/vrc.h"
+#include "engine.h"
+
+#include <cstring>
+#include <memory>
+#include <string>
+
+struct vrc_context {
+  std::unique_ptr<vrc::Engine> eng;
+  std::string err;
+  vrc_timing timing{0.0, 0};
+  std::vector<std::vector<vrc::NodeRecord>> trees;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+using vrc::cplx;
+
+template <class F>
+int guarded(vrc_context* ctx, F&& f) {
+  if (!ctx) return VRC_EINVAL;
+  ctx->err.clear();
+  try {
+    cudaSetDevice(ctx->eng->device());
+    f();
+    return VRC_OK;
+  } catch (const vrc::StatusError& e) {
+    ctx->err = e.what;
+    return e.status;
+  } catch (const vrc::CudaError& e) {
+    ctx->err = std::string("CUDA error: ") + cudaGetErrorString(e.err);
+    return VRC_ECUDA;
+  } catch (const std::bad_alloc&) {
+    ctx->err = "host memory exhausted";
+    return VRC_ENOMEM;
+  } catch (const std::exception& e) {
+    ctx->err = e.what();
+    return VRC_EINVAL;
+  }
+}
+
+struct Timed {
+  vrc_context* ctx;
+  long long l0;
+  explicit Timed(vrc_context* c) : ctx(c), l0(c->eng->launches) {
+    VRC_CUDA_CHECK(cudaEventRecord(ctx->ev0, ctx->eng->stream()));
+  }
+  void done() {
+    VRC_CUDA_CHECK(cudaEventRecord(ctx->ev1, ctx->eng->stream()));
+    VRC_CUDA_CHECK(cudaEventSynchronize(ctx->ev1));
+    float ms = 0.f;
+    VRC_CUDA_CHECK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    ctx->timing.device_ms = ms;
+    ctx->timing.launches = ctx->eng->launches - l0;
+  }
+};
+
+vrc::CellSpec to_spec(const vrc_cell& c) {
+  vrc::CellSpec s;
+  s.kind = c.kind;
+  s.nx = c.nx;
+  s.ny = c.ny;
+  s.pml = c.pml != 0;
+  s.lambda = c.lambda;
+  s.z0 = c.z0;
+  s.z1 = c.z1;
+  if (c.kind == VRC_GEOM_PILLAR) {
+    s.Lx = c.Lx;
+    s.Ly = c.Ly;
+    s.npx = c.npx;
+    s.npy = c.npy;
+    s.eps_in = vrc::mk(c.eps_in.re, c.eps_in.im);
+    s.eps_out = vrc::mk(c.eps_out.re, c.eps_out.im);
+    s.r0 = c.r0;
+    s.r1 = c.r1;
+    if (c.npx < 1 || c.npy < 1 || !(c.Lx > 0) || !(c.Ly > 0))
+      throw vrc::StatusError(VRC_EINVAL, "invalid pillar raster");
+  } else if (c.kind == VRC_GEOM_GRID || c.kind == VRC_GEOM_PIXELS) {
+    if (c.ncx < 2 || c.ncy < 2 || !c.eps) throw vrc::StatusError(VRC_EINVAL, "grid needs ncx, ncy >= 2 and eps");
+    if (c.x) s.x.assign(c.x, c.x + c.ncx);
+    else {
+      if (!(c.Lx > 0)) throw vrc::StatusError(VRC_EINVAL, "missing x coordinates");
+      for (int i = 0; i < c.ncx; ++i) s.x.push_back(c.Lx * i / (c.ncx - 1));
+    }
+    if (c.y) s.y.assign(c.y, c.y + c.ncy);
+    else {
+      if (!(c.Ly > 0)) throw vrc::StatusError(VRC_EINVAL, "missing y coordinates");
+      for (int j = 0; j < c.ncy; ++j) s.y.push_back(c.Ly * j / (c.ncy - 1));
+    }
+    size_t ne = (size_t)(c.ncx - 1) * (c.ncy - 1);
+    s.eps.resize(ne);
+    for (size_t i = 0; i < ne; ++i) s.eps[i] = vrc::mk(c.eps[i].re, c.eps[i].im);
+    for (int i = 0; i < c.n_xrules; ++i) {
+      const vrc_rule& r = c.xrules[i];
+      if (r.nknots < 1 || !r.zs || !r.vals) throw vrc::StatusError(VRC_EINVAL, "invalid x rule");
+      s.xrules.push_back({r.index, std::vector<double>(r.zs, r.zs + r.nknots),
+                          std::vector<double>(r.vals, r.vals + r.nknots)});
+    }
+    for (int i = 0; i < c.n_yrules; ++i) {
+      const vrc_rule& r = c.yrules[i];
+      if (r.nknots < 1 || !r.zs || !r.vals) throw vrc::StatusError(VRC_EINVAL, "invalid y rule");
+      s.yrules.push_back({r.index, std::vector<double>(r.zs, r.zs + r.nknots),
+                          std::vector<double>(r.vals, r.vals + r.nknots)});
+    }
+    if (c.geometry_fn) {
+      vrc_geometry_fn fn = c.geometry_fn;
+      void* user = c.geometry_user;
+      s.geom_cb = [fn, user](double z, double* x, double* y) { fn(user, z, x, y); };
+    }
+  } else {
+    throw vrc::StatusError(VRC_EINVAL, "unknown geometry kind");
+  }
+  s.has_end0 = c.has_end0 != 0;
+  s.has_end1 = c.has_end1 != 0;
+  s.eps_end0 = vrc::mk(c.eps_end0.re, c.eps_end0.im);
+  s.eps_end1 = vrc::mk(c.eps_end1.re, c.eps_end1.im);
+  return s;
+}
+
+std::vector<vrc::CellSpec> to_specs(int ncells, const vrc_cell* cells) {
+  if (ncells < 0 || (ncells > 0 && !cells)) throw vrc::StatusError(VRC_EINVAL, "invalid cell array");
+  std::vector<vrc::CellSpec> v;
+  v.reserve(ncells);
+  for (int i = 0; i < ncells; ++i) v.push_back(to_spec(cells[i]));
+  return v;
+}
+
+void d2h(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  if (dst && src) VRC_CUDA_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+}
+
+void export_results(vrc_context* ctx, std::vector<vrc::CellResult>& res, vrc_result* out) {
+  vrc::Engine& E = *ctx->eng;
+  ctx->trees.clear();
+  for (size_t c = 0; c < res.size(); ++c) {
+    vrc::CellResult& r = res[c];
+    const size_t nn = (size_t)r.n * r.n * 16, nv = (size_t)r.n * 16;
+    if (out) {
+      vrc_result& o = out[c];
+      d2h(o.Tdd, r.Tdd, nn, E.stream());
+      d2h(o.Tuu, r.Tuu, nn, E.stream());
+      d2h(o.Rud, r.Rud, nn, E.stream());
+      d2h(o.Rdu, r.Rdu, nn, E.stream());
+      d2h(o.W0, r.W0, nn, E.stream());
+      d2h(o.V0, r.V0, nn, E.stream());
+      d2h(o.gam0, r.gam0, nv, E.stream());
+      d2h(o.W1, r.W1, nn, E.stream());
+      d2h(o.V1, r.V1, nn, E.stream());
+      d2h(o.gam1, r.gam1, nv, E.stream());
+      o.status = r.status;
+      o.n = r.n;
+      o.N = r.N;
+      o.n_eig = r.n_eig;
+      o.n_samples = r.n_samples;
+      o.n_nodes = r.n_nodes;
+    }
+    ctx->trees.push_back(r.nodes);
+  }
+  E.sync();
+  for (auto& r : res) E.release_result(r);
+}
+}  // namespace
+
+extern "C" {
+
+int vrc_create(int device, vrc_context** ctx) {
+  if (!ctx) return VRC_EINVAL;
+  *ctx = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    (void)cudaGetLastError();
+    return VRC_ENODEV;
+  }
+  if (device < 0 || device >= ndev) return VRC_EINVAL;
+  auto* c = new vrc_context();
+  try {
+    c->eng = std::make_unique<vrc::Engine>(device);
+    VRC_CUDA_CHECK(cudaEventCreate(&c->ev0));
+    VRC_CUDA_CHECK(cudaEventCreate(&c->ev1));
+  } catch (...) {
+    delete c;
+    return VRC_ECUDA;
+  }
+  *ctx = c;
+  return VRC_OK;
+}
+
+void vrc_destroy(vrc_context* ctx) {
+  if (!ctx) return;
+  if (ctx->eng) cudaSetDevice(ctx->eng->device());
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  ctx->eng.reset();
+  delete ctx;
+}
+
+const char* vrc_last_error(const vrc_context* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+const char* vrc_status_string(int s) {
+  switch (s) {
+    case VRC_OK: return "ok";
+    case VRC_EINVAL: return "invalid argument";
+    case VRC_ECUDA: return "CUDA error";
+    case VRC_ENOMEM: return "out of device memory";
+    case VRC_ESINGULAR: return "singular matrix";
+    case VRC_ENOCONV: return "eigensolver did not converge";
+    case VRC_ENONFINITE: return "non-finite value";
+    case VRC_ETIMEOUT: return "timeout";
+    case VRC_EDEPTH: return "maximum recursion depth reached";
+    case VRC_ENODEV: return "no CUDA device";
+    default: return "unknown status";
+  }
+}
+
+int vrc_get_timing(const vrc_context* ctx, vrc_timing* t) {
+  if (!ctx || !t) return VRC_EINVAL;
+  *t = ctx->timing;
+  return VRC_OK;
+}
+
+int vrc_sample_pq(vrc_context* ctx, const vrc_cell* cell, int nz, const double* z, vrc_complex* P, vrc_complex* Q) {
+  return guarded(ctx, [&] {
+    if (!cell || nz < 0 || (nz > 0 && (!z || !P || !Q))) throw vrc::StatusError(VRC_EINVAL, "invalid arguments");
+    vrc::Engine& E = *ctx->eng;
+    vrc::CellSpec s = to_spec(*cell);
+    const int n = s.n();
+    vrc::Engine::CellDev* cd = E.prepare_cell(s);
+    std::vector<cplx*> Pd(nz), Qd(nz);
+    std::vector<vrc::Engine::SampleReq> req;
+    for (int i = 0; i < nz; ++i) {
+      Pd[i] = E.mat(n);
+      Qd[i] = E.mat(n);
+      req.push_back({&s, cd, z[i], false, vrc::mk(1, 0), Pd[i], Qd[i]});
+    }
+    Timed tm(ctx);
+    std::vector<int> st;
+    E.assemble(req, &st);
+    tm.done();
+    for (int i = 0; i < nz; ++i) {
+      d2h(P + (size_t)i * n * n, Pd[i], (size_t)n * n * 16, E.stream());
+      d2h(Q + (size_t)i * n * n, Qd[i], (size_t)n * n * 16, E.stream());
+    }
+    E.sync();
+    for (int i = 0; i < nz; ++i) {
+      E.free_mat(Pd[i], n);
+      E.free_mat(Qd[i], n);
+    }
+    E.release_cell(cd);
+    for (int v : st)
+      if (v) throw vrc::StatusError(v, "assembly reported a singular Toeplitz / eps33 system");
+  });
+}
+
+static int eig_common(vrc_context* ctx, int batch, int n, const vrc_complex* P, const vrc_complex* Q, vrc_complex* W,
+                      vrc_complex* V, vrc_complex* gam, vrc_complex* lam) {
+  return guarded(ctx, [&] {
+    if (batch < 0 || n < 2 || n > 1024 || (batch > 0 && (!P || !W))) throw vrc::StatusError(VRC_EINVAL, "invalid arguments");
+    vrc::Engine& E = *ctx->eng;
+    const size_t nn = (size_t)n * n;
+    std::vector<cplx*> Pd(batch), Qd(batch), Wd(batch), Vd(batch), gd(batch), ld(batch);
+    std::vector<cplx> eye;
+    if (!Q) {
+      eye.assign(nn, vrc::mk(0, 0));
+      for (int i = 0; i < n; ++i) eye[(size_t)i * n + i] = vrc::mk(1, 0);
+    }
+    std::vector<vrc::Engine::EigReq> req;
+    for (int b = 0; b < batch; ++b) {
+      Pd[b] = E.mat(n); Qd[b] = E.mat(n); Wd[b] = E.mat(n); Vd[b] = E.mat(n); gd[b] = E.vec(n); ld[b] = E.vec(n);
+      VRC_CUDA_CHECK(cudaMemcpyAsync(Pd[b], P + (size_t)b * nn, nn * 16, cudaMemcpyHostToDevice, E.stream()));
+      VRC_CUDA_CHECK(cudaMemcpyAsync(Qd[b], Q ? (const void*)(Q + (size_t)b * nn) : (const void*)eye.data(), nn * 16,
+                                     cudaMemcpyHostToDevice, E.stream()));
+      vrc::Engine::EigReq r{Pd[b], Qd[b], Wd[b], Vd[b], nullptr, nullptr, gd[b]};
+      r.lam = ld[b];
+      req.push_back(r);
+    }
+    Timed tm(ctx);
+    std::vector<int> st;
+    E.eig(req, n, &st);
+    tm.done();
+    for (int b = 0; b < batch; ++b) {
+      d2h(W + (size_t)b * nn, Wd[b], nn * 16, E.stream());
+      if (V) d2h(V + (size_t)b * nn, Vd[b], nn * 16, E.stream());
+      if (gam) d2h(gam + (size_t)b * n, gd[b], (size_t)n * 16, E.stream());
+      if (lam) d2h(lam + (size_t)b * n, ld[b], (size_t)n * 16, E.stream());
+    }
+    E.sync();
+    for (int b = 0; b < batch; ++b) {
+      E.free_mat(Pd[b], n); E.free_mat(Qd[b], n); E.free_mat(Wd[b], n); E.free_mat(Vd[b], n);
+      E.free_vec(gd[b], n); E.free_vec(ld[b], n);
+    }
+    for (int v : st)
+      if (v) throw vrc::StatusError(v, "eigensolver failure");
+  });
+}
+
+int vrc_wave_solve(vrc_context* ctx, int batch, int n, const vrc_complex* P, const vrc_complex* Q, vrc_complex* W,
+                   vrc_complex* V, vrc_complex* gam) {
+  if (!Q) return VRC_EINVAL;
+  return eig_common(ctx, batch, n, P, Q, W, V, gam, nullptr);
+}
+
+int vrc_eig(vrc_context* ctx, int batch, int n, const vrc_complex* A, vrc_complex* W, vrc_complex* lam) {
+  return eig_common(ctx, batch, n, A, nullptr, W, nullptr, nullptr, lam);
+}
+
+int vrc_redheffer(vrc_context* ctx, int ncells, const vrc_cell* cells, double pe, int max_depth, vrc_result* results) {
+  return guarded(ctx, [&] {
+    if (!(pe > 0.0) || max_depth < 0) throw vrc::StatusError(VRC_EINVAL, "pe must be > 0 and max_depth >= 0");
+    auto specs = to_specs(ncells, cells);
+    vrc::Engine::RedhefferOpts o;
+    o.pe = pe;
+    o.max_depth = max_depth;
+    std::vector<vrc::CellResult> res;
+    Timed tm(ctx);
+    ctx->eng->redheffer(specs, o, res);
+    tm.done();
+    export_results(ctx, res, results);
+  });
+}
+
+int vrc_redheffer_segments(vrc_context* ctx, int ncells, const vrc_cell* cells, const int* ncuts,
+                           const double* const* cuts, vrc_result* results) {
+  return guarded(ctx, [&] {
+    auto specs = to_specs(ncells, cells);
+    if (ncells > 0 && (!ncuts || !cuts)) throw vrc::StatusError(VRC_EINVAL, "missing cuts");
+    std::vector<std::vector<double>> cv(ncells);
+    for (int c = 0; c < ncells; ++c) {
+      if (ncuts[c] < 2 || !cuts[c]) throw vrc::StatusError(VRC_EINVAL, "each cell needs >= 2 cut points");
+      cv[c].assign(cuts[c], cuts[c] + ncuts[c]);
+      for (int k = 0; k + 1 < ncuts[c]; ++k)
+        if (!(cv[c][k + 1] > cv[c][k])) throw vrc::StatusError(VRC_EINVAL, "cut points must increase");
+      specs[c].z0 = cv[c].front();
+      specs[c].z1 = cv[c].back();
+    }
+    vrc::Engine::RedhefferOpts o;
+    o.cuts = &cv;
+    std::vector<vrc::CellResult> res;
+    Timed tm(ctx);
+    ctx->eng->redheffer(specs, o, res);
+    tm.done();
+    export_results(ctx, res, results);
+  });
+}
+
+int vrc_get_tree(vrc_context* ctx, int cell, int max_nodes, double* a, double* b, double* err, int* accepted) {
+  if (!ctx || cell < 0 || cell >= (int)ctx->trees.size()) return -VRC_EINVAL;
+  const auto& t = ctx->trees[cell];
+  for (int i = 0; i < (int)t.size() && i < max_nodes; ++i) {
+    if (a) a[i] = t[i].a;
+    if (b) b[i] = t[i].b;
+    if (err) err[i] = t[i].err;
+    if (accepted) accepted[i] = t[i].accepted;
+  }
+  return (int)t.size();
+}
+
+int vrc_rcwa(vrc_context* ctx, int ncells, const vrc_cell* cells, int N, vrc_result* results) {
+  return guarded(ctx, [&] {
+    auto specs = to_specs(ncells, cells);
+    std::vector<vrc::CellResult> res;
+    Timed tm(ctx);
+    ctx->eng->rcwa(specs, N, res);
+    tm.done();
+    export_results(ctx, res, results);
+  });
+}
+
+int vrc_differential(vrc_context* ctx, int ncells, const vrc_cell* cells, int N, vrc_result* results) {
+  return guarded(ctx, [&] {
+    auto specs = to_specs(ncells, cells);
+    std::vector<vrc::CellResult> res;
+    Timed tm(ctx);
+    ctx->eng->differential(specs, N, res);
+    tm.done();
+    export_results(ctx, res, results);
+  });
+}
+
+int vrc_order_powers(vrc_context* ctx, int ncells, const vrc_cell* cells, int method, double pe, int max_depth,
+                     int nslices, int side, int flux_norm, double* R, double* T, int* status) {
+  return guarded(ctx, [&] {
+    if (!R || !T || (side != 0 && side != 1)) throw vrc::StatusError(VRC_EINVAL, "invalid arguments");
+    auto specs = to_specs(ncells, cells);
+    vrc::Engine& E = *ctx->eng;
+    std::vector<vrc::CellResult> res;
+    Timed tm(ctx);
+    if (method == 0) {
+      if (!(pe > 0.0)) throw vrc::StatusError(VRC_EINVAL, "pe must be > 0");
+      vrc::Engine::RedhefferOpts o;
+      o.pe = pe;
+      o.max_depth = max_depth;
+      E.redheffer(specs, o, res);
+    } else if (method == 1) {
+      E.rcwa(specs, nslices, res);
+    } else if (method == 2) {
+      E.differential(specs, nslices, res);
+    } else {
+      throw vrc::StatusError(VRC_EINVAL, "unknown method");
+    }
+    std::vector<std::vector<double>> Rv, Tv;
+    E.order_powers(specs, res, side, flux_norm, Rv, Tv);
+    tm.done();
+    size_t off = 0;
+    for (int c = 0; c < ncells; ++c) {
+      std::memcpy(R + off, Rv[c].data(), Rv[c].size() * sizeof(double));
+      std::memcpy(T + off, Tv[c].data(), Tv[c].size() * sizeof(double));
+      off += Rv[c].size();
+      if (status) status[c] = res[c].status;
+    }
+    ctx->trees.clear();
+    for (auto& r : res) {
+      ctx->trees.push_back(r.nodes);
+      E.release_result(r);
+    }
+  });
+}
+
+int vrc_zgemm(vrc_context* ctx, int batch, int n, const vrc_complex* A, const vrc_complex* B, vrc_complex* C) {
+  return guarded(ctx, [&] {
+    if (batch < 0 || n < 1 || (batch > 0 && (!A || !B || !C))) throw vrc::StatusError(VRC_EINVAL, "invalid arguments");
+    vrc::Engine& E = *ctx->eng;
+    const size_t nn = (size_t)n * n;
+    std::vector<vrc::GemmDesc> g;
+    std::vector<cplx*> bufs;
+    for (int b = 0; b < batch; ++b) {
+      cplx *a = E.mat(n), *bb = E.mat(n), *c = E.mat(n);
+      bufs.insert(bufs.end(), {a, bb, c});
+      VRC_CUDA_CHECK(cudaMemcpyAsync(a, A + b * nn, nn * 16, cudaMemcpyHostToDevice, E.stream()));
+      VRC_CUDA_CHECK(cudaMemcpyAsync(bb, B + b * nn, nn * 16, cudaMemcpyHostToDevice, E.stream()));
+      g.push_back({a, bb, c, nullptr, nullptr, nullptr});
+    }
+    Timed tm(ctx);
+    E.gemm(g, n, vrc::mk(1, 0), vrc::mk(0, 0), 0.0);
+    tm.done();
+    for (int b = 0; b < batch; ++b) d2h(C + b * nn, g[b].C, nn * 16, E.stream());
+    E.sync();
+    for (auto* p : bufs) E.free_mat(p, n);
+  });
+}
+
+int vrc_zinv(vrc_context* ctx, int batch, int n, vrc_complex* A, int* status) {
+  return guarded(ctx, [&] {
+    if (batch < 0 || n < 1 || (batch > 0 && !A)) throw vrc::StatusError(VRC_EINVAL, "invalid arguments");
+    vrc::Engine& E = *ctx->eng;
+    const size_t nn = (size_t)n * n;
+    std::vector<cplx*> m(batch);
+    for (int b = 0; b < batch; ++b) {
+      m[b] = E.mat(n);
+      VRC_CUDA_CHECK(cudaMemcpyAsync(m[b], A + b * nn, nn * 16, cudaMemcpyHostToDevice, E.stream()));
+    }
+    std::vector<int> st;
+    Timed tm(ctx);
+    E.inverse(m, n, &st);
+    tm.done();
+    for (int b = 0; b < batch; ++b) d2h(A + b * nn, m[b], nn * 16, E.stream());
+    E.sync();
+    for (int b = 0; b < batch; ++b) {
+      E.free_mat(m[b], n);
+      if (status) status[b] = b < (int)st.size() ? st[b] : 0;
+    }
+  });
+}
+
+}  // extern "C"

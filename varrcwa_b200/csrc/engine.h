@@ -1,0 +1,262 @@
+// Host engine: memory pools, descriptor staging and the batched stages of
+// the varRCWA hot path, driven from C++ (no host-side math on the path).
+#pragma once
+
+#include <functional>
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace vrc {
+
+enum GeomKind { GEOM_GRID = 0, GEOM_PILLAR = 1, GEOM_PIXELS = 2 };
+
+struct PwlRule {
+  int index;
+  std::vector<double> zs, vals;
+  double eval(double z) const;
+};
+
+// Geometry + optics of one structure (one "cell" of a batch).
+struct CellSpec {
+  int kind = GEOM_GRID;
+  int nx = 1, ny = 1;
+  bool pml = false;
+  double lambda = 1.0;
+  double z0 = 0.0, z1 = 1.0;
+  // grid / pixels
+  std::vector<double> x, y;
+  std::vector<cplx> eps;  // (ncy-1) x (ncx-1), row-major (rows = y strips)
+  std::vector<PwlRule> xrules, yrules;
+  std::function<void(double, double*, double*)> geom_cb;  // optional host rule callback
+  // pillar
+  double Lx = 1.0, Ly = 1.0;
+  int npx = 0, npy = 0;
+  cplx eps_in{1.0, 0.0}, eps_out{1.0, 0.0};
+  double r0 = 0.0, r1 = 0.0;
+  // homogeneous end media (otherwise the structure's own bases at z0/z1)
+  bool has_end0 = false, has_end1 = false;
+  cplx eps_end0{1.0, 0.0}, eps_end1{1.0, 0.0};
+
+  int ncx() const { return kind == GEOM_PILLAR ? npx + 1 : (int)x.size(); }
+  int ncy() const { return kind == GEOM_PILLAR ? npy + 1 : (int)y.size(); }
+  int m() const { return nx * ny; }
+  int n() const { return 2 * nx * ny; }
+  double k0() const { return 2.0 * 3.1415926535897932 / lambda; }
+  void geometry(double z, std::vector<double>& xo, std::vector<double>& yo) const;
+  double radius(double z) const;
+};
+
+struct NodeRecord {
+  double a, b, err;
+  int accepted;
+};
+
+struct CellResult {
+  int status = ST_OK;
+  int n = 0;
+  int N = 0;          // accepted segments / slices
+  int n_eig = 0;      // eigen-decompositions performed
+  int n_samples = 0;  // P,Q samples assembled
+  int n_nodes = 0;    // segments evaluated (accepted + rejected)
+  // device-resident results (owned by the engine until released)
+  cplx *Tdd = nullptr, *Tuu = nullptr, *Rud = nullptr, *Rdu = nullptr;
+  cplx *W0 = nullptr, *V0 = nullptr, *gam0 = nullptr, *W0inv = nullptr;
+  cplx *W1 = nullptr, *V1 = nullptr, *gam1 = nullptr, *W1inv = nullptr;
+  std::vector<NodeRecord> nodes;
+};
+
+// Fixed-size device block pool.
+class BlockPool {
+ public:
+  explicit BlockPool(size_t bytes) : bytes_(bytes) {}
+  ~BlockPool();
+  void* get();
+  void put(void* p) { free_.push_back(p); }
+  size_t bytes() const { return bytes_; }
+
+ private:
+  size_t bytes_;
+  std::vector<void*> free_;
+  std::vector<void*> chunks_;
+};
+
+class Engine {
+ public:
+  explicit Engine(int device);
+  ~Engine();
+  Engine(const Engine&) = delete;
+  Engine& operator=(const Engine&) = delete;
+
+  int device() const { return device_; }
+  cudaStream_t stream() const { return stream_; }
+  void set_stream(cudaStream_t s) { stream_ = s; }
+  void sync();
+
+  // memory
+  cplx* mat(int n);
+  cplx* vec(int n);
+  void free_mat(cplx* p, int n);
+  void free_vec(cplx* p, int n);
+  void* bytes(size_t b);
+  void free_bytes(void* p, size_t b);
+  template <class T>
+  T* upload(const T* data, size_t count);
+  template <class T>
+  T* upload(const std::vector<T>& v) {
+    return upload(v.data(), v.size());
+  }
+  void* workspace(size_t bytes);
+  size_t batch_budget_bytes() const;
+
+  // batched primitives
+  void gemm(std::vector<GemmDesc>& d, int n, cplx alpha, cplx beta, double delta);
+  void inverse(const std::vector<cplx*>& mats, int n, std::vector<int>* status);
+  void copy(const std::vector<cplx*>& src, const std::vector<cplx*>& dst, int n);
+  void axpby(const std::vector<const cplx*>& A, const std::vector<const cplx*>& B, const std::vector<cplx*>& C,
+             cplx alpha, cplx beta, double delta, int n);
+
+  // ---- stages ----
+  // Per-cell constant data (K matrices).
+  struct CellDev {
+    int nx, ny, m, n;
+    double k0;
+    bool pml;
+    double* alpha = nullptr;  // device (m)
+    double* beta = nullptr;
+    std::vector<double> h_alpha, h_beta;
+    cplx *Kx = nullptr, *Ky = nullptr, *KxKy = nullptr, *KxKx = nullptr, *KyKy = nullptr, *KyKx = nullptr;
+    cplx* eps_dev = nullptr;  // fixed permittivity table (grid / pixels)
+    size_t eps_count = 0;
+  };
+  CellDev* prepare_cell(const CellSpec& c);
+  void release_cell(CellDev* cd);
+
+  struct SampleReq {
+    const CellSpec* spec;
+    CellDev* cd;
+    double z;
+    bool homogeneous;  // sample a homogeneous medium eps_h instead of the structure
+    cplx eps_h;
+    cplx* P;
+    cplx* Q;
+  };
+  void assemble(std::vector<SampleReq>& reqs, std::vector<int>* status);
+
+  struct EigReq {
+    const cplx* P;
+    const cplx* Q;
+    cplx *W, *V, *Winv, *Vinv, *gam;
+    cplx* lam = nullptr;  // optional copy of the eigenvalues of P*Q
+  };
+  void eig(std::vector<EigReq>& reqs, int n, std::vector<int>* status);
+
+  struct SegReq {
+    const cplx *Pr, *Qr, *W, *V, *Winv, *Vinv, *gam;
+    const cplx *Pa, *Qa, *Pb, *Qb;
+    double z0, z1, k0;
+    cplx *tdd, *tuu, *rud, *rdu;
+    double* err;  // device
+  };
+  void segments(std::vector<SegReq>& reqs, int n);
+
+  // Left-end re-expression of segment blocks from the basis (Winv,Vinv) of
+  // the segment into (leftW, leftV).  Blocks updated in place.
+  struct ProjReq {
+    const cplx *Winv, *Vinv, *leftW, *leftV;
+    cplx *tdd, *tuu, *rud, *rdu;
+  };
+  void project_left(std::vector<ProjReq>& reqs, int n, std::vector<int>* status);
+  // Right-end re-expression: S's right end from basis (leftWinv,leftVinv) to (W1,V1).
+  struct ProjRReq {
+    const cplx *leftWinv, *leftVinv, *W1, *V1;
+    cplx *Tdd, *Tuu, *Rud, *Rdu;
+  };
+  void project_right(std::vector<ProjRReq>& reqs, int n, std::vector<int>* status);
+  // RCWA-style left-end projection: chain expressed in (W1,V1) on both ends,
+  // left end moved to (W0,V0); W1inv, V1inv given.
+  struct ProjLEReq {
+    const cplx *W1inv, *V1inv, *W0, *V0;
+    cplx *Tdd, *Tuu, *Rud, *Rdu;
+  };
+  void project_left_end(std::vector<ProjLEReq>& reqs, int n, std::vector<int>* status);
+
+  // Star product: out = L * R (L on the z0 side).  Out buffers must not
+  // alias the inputs.
+  struct StarReq {
+    const cplx *Tdd, *Tuu, *Rud, *Rdu;  // left (accumulated)
+    const cplx *tdd, *tuu, *rud, *rdu;  // right (new)
+    cplx *oTdd, *oTuu, *oRud, *oRdu;
+  };
+  void star(std::vector<StarReq>& reqs, int n, std::vector<int>* status);
+
+  // Reduce per-cell ordered lists of S-matrices (4 blocks each) to one per
+  // cell by pairwise star products.  Inputs are consumed (freed) except the
+  // final survivor, returned in place of lists[c][0].
+  struct SBlocks {
+    cplx *tdd, *tuu, *rud, *rdu;
+  };
+  void star_reduce(std::vector<std::vector<SBlocks>>& lists, int n, std::vector<int>* cell_status);
+
+  // RCWA slab S-matrix (tuu, rud) in the basis (W1, V1) for samples P,Q.
+  struct SlabReq {
+    const cplx *P, *Q, *W1, *V1;
+    double k0, dz;
+    cplx *tuu, *rud;
+  };
+  void rcwa_slabs(std::vector<SlabReq>& reqs, int n, std::vector<int>* status);
+
+  // Differential-method slice from samples at (zl, zm, zr).
+  struct DiffReq {
+    const cplx *P0, *Q0, *P1, *Q1, *P2, *Q2;
+    const cplx *W1, *V1, *W1inv, *V1inv;
+    double k0, dz;
+    cplx *tdd, *tuu, *rud, *rdu;
+  };
+  void diff_slices(std::vector<DiffReq>& reqs, int n, std::vector<int>* status);
+
+  // ---- drivers ----
+  struct RedhefferOpts {
+    double pe = 1e-2;
+    int max_depth = 40;
+    const std::vector<std::vector<double>>* cuts = nullptr;  // explicit segments (replay)
+  };
+  void redheffer(const std::vector<CellSpec>& cells, const RedhefferOpts& o, std::vector<CellResult>& out);
+  void rcwa(const std::vector<CellSpec>& cells, int N, std::vector<CellResult>& out);
+  void differential(const std::vector<CellSpec>& cells, int N, std::vector<CellResult>& out);
+  void release_result(CellResult& r);
+
+  // Per-order powers for the two polarisations (px,py) = (1,0), (0,1).
+  // side 0: incidence from z0 (Rdu, Tuu), 1: from z1 (Rud, Tdd).
+  void order_powers(const std::vector<CellSpec>& cells, const std::vector<CellResult>& res, int side,
+                    int flux_norm, std::vector<std::vector<double>>& R, std::vector<std::vector<double>>& T);
+
+  // counters
+  long long launches = 0;
+
+ private:
+  int device_;
+  cudaStream_t stream_;
+  bool own_stream_;
+  std::map<size_t, std::unique_ptr<BlockPool>> pools_;
+  char* h_stage_ = nullptr;
+  char* d_stage_ = nullptr;
+  size_t stage_cap_ = 0, stage_off_ = 0;
+  void* ws_ = nullptr;
+  size_t ws_cap_ = 0;
+  BlockPool& pool(size_t bytes);
+  void* stage(const void* data, size_t bytes);
+  struct EndBasis {
+    cplx *W, *V, *Winv, *Vinv, *gam;
+  };
+};
+
+template <class T>
+T* Engine::upload(const T* data, size_t count) {
+  return reinterpret_cast<T*>(stage(data, count * sizeof(T)));
+}
+
+}  // namespace vrc

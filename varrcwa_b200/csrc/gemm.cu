@@ -1,0 +1,173 @@
+// Batched complex128 GEMM on FP64 tensor cores (DMMA, mma.sync m16n8k4 f64).
+//
+//   C = diag(rs) * (alpha * A * B) * diag(cs) + beta * Cin + delta * I
+//
+// for square column-major n x n operands (every contraction of the hot path
+// is square: projections, star products, perturbation terms, P*Q).  One CTA
+// computes a 64 x 64 complex tile; operands are staged through shared memory
+// by 16-byte cp.async copies in a 3-stage pipeline.  The complex product is
+// the 4-real-product form (Cr += Ar Br - Ai Bi, Ci += Ar Bi + Ai Br), which
+// keeps the rounding of a standard complex GEMM (cuBLAS Zgemm3m used by the
+// reference GPU path, src/gpu/types.cuh:33, changes rounding; Eigen/MKL on
+// the CPU path do not).
+#include "common.cuh"
+#include "kernels.h"
+
+namespace vrc {
+
+namespace {
+
+constexpr int BM = 64, BN = 64, BK = 8, STAGES = 3;
+constexpr int LDA = BM + 2;  // complex elements per k-row of the A tile
+constexpr int LDB = BN + 2;
+constexpr int NTHREADS = 256;
+constexpr int SMEM_BYTES = STAGES * BK * (LDA + LDB) * 16;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  int sz = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, double b0) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+      "{%0,%1,%2,%3};\n"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a0), "d"(a1), "d"(b0));
+}
+
+__global__ void __launch_bounds__(NTHREADS)
+    zgemm_kernel(const GemmDesc* __restrict__ descs, int n, cplx alpha, cplx beta, double delta) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx* As = reinterpret_cast<cplx*>(smem_raw);        // [STAGES][BK][LDA]
+  cplx* Bs = As + STAGES * BK * LDA;                    // [STAGES][BK][LDB]
+
+  const GemmDesc d = descs[blockIdx.y];
+  const int tiles_m = (n + BM - 1) / BM;
+  const int m0 = (blockIdx.x % tiles_m) * BM;
+  const int n0 = (blockIdx.x / tiles_m) * BN;
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, tig = lane & 3;
+  const int wm = warp & 1, wn = warp >> 1;  // 2 x 4 warps, 32 x 16 complex each
+
+  const cplx* __restrict__ A = d.A;
+  const cplx* __restrict__ B = d.B;
+  const int KT = (n + BK - 1) / BK;
+
+  auto load_tile = [&](int stage, int kt) {
+    const int k0 = kt * BK;
+    cplx* as = As + stage * BK * LDA;
+    cplx* bs = Bs + stage * BK * LDB;
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      int idx = tid + i * NTHREADS;
+      // A tile: 64 rows x 8 cols, consecutive threads -> consecutive rows.
+      int r = idx & 63, k = idx >> 6;
+      int gr = m0 + r, gk = k0 + k;
+      bool va = (gr < n) && (gk < n);
+      cp_async16(as + k * LDA + r, va ? (const void*)(A + (size_t)gk * n + gr) : (const void*)A, va);
+      // B tile: 8 rows x 64 cols, consecutive threads -> consecutive k.
+      int kb = idx & 7, c = idx >> 3;
+      int gkb = k0 + kb, gc = n0 + c;
+      bool vb = (gkb < n) && (gc < n);
+      cp_async16(bs + kb * LDB + c, vb ? (const void*)(B + (size_t)gc * n + gkb) : (const void*)B, vb);
+    }
+  };
+
+  double acc_r[2][2][4], acc_i[2][2][4];
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) acc_r[a][b][c] = acc_i[a][b][c] = 0.0;
+
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < KT) load_tile(s, s);
+    cp_async_commit();
+  }
+
+  for (int kt = 0; kt < KT; ++kt) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    int nk = kt + STAGES - 1;
+    if (nk < KT) load_tile(nk % STAGES, nk);
+    cp_async_commit();
+
+    const cplx* as = As + (kt % STAGES) * BK * LDA;
+    const cplx* bs = Bs + (kt % STAGES) * BK * LDB;
+#pragma unroll
+    for (int ks = 0; ks < BK; ks += 4) {
+      cplx af[2][2], bf[2];
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt) {
+        int row = wm * 32 + mt * 16 + g;
+        af[mt][0] = as[(ks + tig) * LDA + row];
+        af[mt][1] = as[(ks + tig) * LDA + row + 8];
+      }
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt) bf[nt] = bs[(ks + tig) * LDB + wn * 16 + nt * 8 + g];
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) {
+          dmma(acc_r[mt][nt], af[mt][0].x, af[mt][1].x, bf[nt].x);
+          dmma(acc_r[mt][nt], -af[mt][0].y, -af[mt][1].y, bf[nt].y);
+          dmma(acc_i[mt][nt], af[mt][0].x, af[mt][1].x, bf[nt].y);
+          dmma(acc_i[mt][nt], af[mt][0].y, af[mt][1].y, bf[nt].x);
+        }
+    }
+  }
+  cp_async_wait<0>();
+
+  // Epilogue.
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        int row = m0 + wm * 32 + mt * 16 + g + ((c >> 1) << 3);
+        int col = n0 + wn * 16 + nt * 8 + tig * 2 + (c & 1);
+        if (row < n && col < n) {
+          cplx v = mk(acc_r[mt][nt][c], acc_i[mt][nt][c]);
+          v = cmul(alpha, v);
+          if (d.rs) v = cmul(d.rs[row], v);
+          if (d.cs) v = cmul(v, d.cs[col]);
+          size_t off = (size_t)col * n + row;
+          if (d.Cin) v = cfma(beta, d.Cin[off], v);
+          if (row == col) v.x += delta;
+          d.C[off] = v;
+        }
+      }
+}
+
+}  // namespace
+
+void zgemm_batched(const GemmDesc* d_descs, int batch, int n, cplx alpha, cplx beta, double delta,
+                   cudaStream_t stream) {
+  static bool configured = false;
+  if (!configured) {
+    VRC_CUDA_CHECK(cudaFuncSetAttribute(zgemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        SMEM_BYTES));
+    configured = true;
+  }
+  if (batch <= 0) return;
+  int tiles = ((n + BM - 1) / BM) * ((n + BN - 1) / BN);
+  for (int b0 = 0; b0 < batch; b0 += 65535) {
+    int nb = batch - b0 < 65535 ? batch - b0 : 65535;
+    dim3 grid(tiles, nb);
+    zgemm_kernel<<<grid, NTHREADS, SMEM_BYTES, stream>>>(d_descs + b0, n, alpha, beta, delta);
+  }
+  VRC_CUDA_CHECK(cudaGetLastError());
+}
+
+}  // namespace vrc

@@ -1,0 +1,94 @@
+// Host-side launchers of the device kernels (internal interface of the
+// engine; the public boundary is include/vrc.h).
+#pragma once
+
+#include "common.cuh"
+
+namespace vrc {
+
+// ---- GEMM: C = diag(rs) (alpha A B) diag(cs) + beta Cin + delta I -----------
+struct GemmDesc {
+  const cplx* A;
+  const cplx* B;
+  cplx* C;
+  const cplx* Cin;  // may be null (beta ignored) or alias C
+  const cplx* rs;   // optional row scale (n)
+  const cplx* cs;   // optional column scale (n)
+};
+void zgemm_batched(const GemmDesc* d_descs, int batch, int n, cplx alpha, cplx beta, double delta,
+                   cudaStream_t stream);
+
+// ---- inverse (in place) -------------------------------------------------------
+int zinv_panel_width(int n);
+void zinv_batched(cplx* const* d_mats, int batch, int n, int* d_status, cudaStream_t stream);
+
+// ---- eigensolver ---------------------------------------------------------------
+void hessenberg_batched(cplx* const* d_H, cplx* const* d_Z, int batch, int n, cudaStream_t st);
+void schur_batched(cplx* const* d_H, cplx* const* d_Z, cplx* const* d_W, int batch, int n, int* d_status,
+                   cudaStream_t st);
+void trevc_batched(cplx* const* d_T, cplx* const* d_Y, int batch, int n, cudaStream_t st);
+void vecnorm_batched(cplx* const* d_X, int batch, int n, cudaStream_t st);
+
+// ---- assembly -------------------------------------------------------------------
+void pillar_raster(const double* d_radius, cplx* const* d_eps, int batch, int npx, int npy, double Lx,
+                   double Ly, cplx eps_in, cplx eps_out, cudaStream_t st);
+void twiddles(const double* const* d_coords, cplx* const* d_out, int batch, int ncoord, int P, cudaStream_t st);
+void reciprocal(cplx* const* d_in, cplx* const* d_out, int batch, int total, cudaStream_t st);
+void small_gemm(int M, int N, int K, const cplx* const* d_A, int lda, const cplx* const* d_B, int ldb, int transB,
+                cplx* const* d_C, int ldc, int batch, cudaStream_t st);
+void toeplitz_inverses(const cplx* const* d_F, cplx* const* d_out, int t, int nmat, int batch, int* d_status,
+                       cudaStream_t st);
+void gather_fe(const cplx* const* d_G11, const cplx* const* d_G22, const cplx* const* d_F2, cplx* const* d_fe11,
+               cplx* const* d_fe22, cplx* const* d_fe33, int nx, int ny, int batch, cudaStream_t st);
+void assemble_periodic(const cplx* const* d_finv, const cplx* const* d_fe11, const cplx* const* d_fe22,
+                       const double* d_alpha, const double* d_beta, const double* d_k0sq, cplx* const* d_P,
+                       cplx* const* d_Q, int m, int batch, cudaStream_t st);
+void assemble_dense(const cplx* const* KxF2h, const cplx* const* KxF1h, const cplx* const* KyF2h,
+                    const cplx* const* KyF1h, const cplx* const* fe11, const cplx* const* fe22, const cplx* KxKy,
+                    const cplx* KxKx, const cplx* KyKy, const cplx* KyKx, const double* d_k0sq, cplx* const* d_P,
+                    cplx* const* d_Q, int m, int batch, cudaStream_t st);
+
+// ---- segment / elementwise ------------------------------------------------------
+struct SegDesc {
+  const cplx* X0;
+  const cplx* Y0;
+  const cplx* X2;
+  const cplx* Y2;
+  const cplx* gam;
+  cplx* tdd;
+  cplx* tuu;
+  cplx* rud;
+  cplx* rdu;
+  double* err;
+  double z0, z1, k0;
+};
+struct PowerDesc {
+  const cplx* r;  // reflected harmonics [rx; ry] (2m)
+  const cplx* t;  // transmitted harmonics [tx; ty]
+  const double* alpha;
+  const double* beta;
+  double* R;
+  double* T;
+  cplx eps_in, eps_out;
+  double k0, tnorm;
+};
+struct MatVecDesc {
+  const cplx* A;
+  const cplx* x;
+  cplx* y;
+};
+void gamma_batched(const cplx* const* lams, cplx* const* gams, cplx* const* invgams, int batch, int n,
+                   cudaStream_t st);
+void sub_batched(const cplx* const* A, const cplx* const* B, cplx* const* C, int batch, long long total,
+                 cudaStream_t st);
+void ab_batched(cplx* const* F, cplx* const* G, int batch, long long total, cudaStream_t st);
+void simpson_batched(const SegDesc* d_segs, int batch, int n, cudaStream_t st);
+void phase_rows_batched(const cplx* const* A, const cplx* const* gam, const double* t, cplx* const* out, int batch,
+                        int n, cudaStream_t st);
+void set_identity_batched(cplx* const* A, int batch, int n, double diag, cudaStream_t st);
+void axpby_batched(const cplx* const* A, const cplx* const* B, cplx* const* C, cplx alpha, cplx beta, double delta,
+                   int batch, int n, cudaStream_t st);
+void order_power_batched(const PowerDesc* d, int batch, int m, cudaStream_t st);
+void matvec_batched(const MatVecDesc* d, int batch, int n, cudaStream_t st);
+
+}  // namespace vrc
