@@ -1,0 +1,334 @@
+#!/usr/bin/env python
+"""Benchmark of the batched varRCWA S-matrix solve on B200.
+
+Workload (default): a batch of config-2 pillar unit cells -- 400 nm square
+period, 532 nm, 11x11 orders (n = 242, complex128), a tapered circular
+pillar (eps 5.8) of height 600 nm with seeded base radius U[60,140] nm and
+sidewall angle U[85,90] deg, rasterised on 256x256 pixels per z-sample, on
+an SiO2 substrate (eps 2.13) under air -- each solved by adaptive varRCWA
+(pe = 1e-2) and reduced to per-order reflected/transmitted power for both
+polarisations.  A step is one batched call of the C-ABI on `--batch` cells.
+
+Metric: S-matrix solves per second (whole job, all ranks).  `value` is the
+device time of the calls (CUDA events on the engine stream); `e2e` is the
+wall time of the same C-ABI calls from host structure descriptors to host
+order powers.  Multi-GPU runs are independent replicas (one process per
+GPU, disjoint cell seeds, no collective on the data path).
+
+`--impl reference` times the CPU restatement of the reference algorithm
+(the oracle) on this machine's host cores on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--batch", type=int, default=64, help="cells per step per GPU")
+    p.add_argument("--workload", default="c2", choices=["c2", "c3"])
+    p.add_argument("--pe", type=float, default=1e-2)
+    p.add_argument("--npix", type=int, default=256)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-cells", type=int, default=1, help="cells in the bounded CPU sample")
+    return p.parse_args()
+
+
+def make_cells(workload, batch, rank, npix, step_seed=0):
+    from varrcwa_b200 import structures as st
+    base = 1000 * (2 if workload == "c2" else 3) + 100000 * rank + step_seed
+    if workload == "c2":
+        return [st.pillar_config2(seed=base + i, npix=npix) for i in range(batch)]
+    return [st.pillar_config3(seed=base + i, npix=npix) for i in range(batch)]
+
+
+# ---------------------------------------------------------------------------
+# clocks sampling during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        sm.sort()
+        med = sm[len(sm) // 2] if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def dgemm_peak_tflops(device):
+    """Measured FP64 tensor-core throughput of cuBLAS DGEMM (torch float64
+    matmul, 8192^3, best of 5) on this GPU: the denominator for the FP64
+    DMMA GEMM roofline (no FP64 figure is driver-measured)."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=device)
+    b = torch.randn(n, n, dtype=torch.float64, device=device)
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize(device)
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        a @ b
+        e1.record()
+        torch.cuda.synchronize(device)
+        ms = e0.elapsed_time(e1)
+        best = max(best, 2.0 * n ** 3 / (ms * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+# ---------------------------------------------------------------------------
+# CPU arms (oracle = CPU restatement of the reference algorithm)
+# ---------------------------------------------------------------------------
+def _oracle_cell(args):
+    desc, pe = args
+    from oracle import varrcwa_oracle as O
+    from oracle.structures_adapter import end_bases, make_sampler
+    s = make_sampler(desc)
+    e0, e1 = end_bases(desc, s)
+    S = O.redheffer_compute(s, desc["z0"], desc["z1"], pe=pe, end0=e0, end1=e1)
+    R, T = O.order_powers(S, s, desc["end1"], desc["end0"], 1.0, 0.0, side="top")
+    return float(R.sum() + T.sum())
+
+
+def cpu_sample(descs, pe):
+    """Time the oracle on the given cells with all host threads (BLAS)."""
+    t0 = time.perf_counter()
+    for d in descs:
+        _oracle_cell((d, pe))
+    return time.perf_counter() - t0
+
+
+def run_reference(a, rank, world):
+    import multiprocessing as mp
+    if world > 1 and rank != 0:
+        return  # rank 0 alone times the CPU reference
+    ncores = os.cpu_count() or 1
+    workers = max(1, ncores)
+    descs = make_cells(a.workload, workers, rank, a.npix)
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    os.environ["OMP_NUM_THREADS"] = "1"
+    os.environ["MKL_NUM_THREADS"] = "1"
+    ctxm = mp.get_context("spawn")
+    with ctxm.Pool(workers) as pool:
+        # warm-up: one small task per worker (imports, first BLAS call)
+        for _ in range(a.warmup):
+            pool.map(_oracle_cell, [(d, 0.5) for d in make_cells(a.workload, workers, rank, 16)])
+        t0 = time.perf_counter()
+        for _ in range(a.steps):
+            pool.map(_oracle_cell, [(d, a.pe) for d in descs])
+        dt = time.perf_counter() - t0
+    value = a.steps * len(descs) / dt
+    line = {
+        "impl": "reference", "metric": metric_name(), "value": value, "unit": "solves/s", "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * dt / a.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "complex128", "data": "synthetic",
+        "config": workload_config(a, len(descs)),
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": workers, "kind": "port",
+                         "sample": f"{len(descs)} cells per step, one per process (spawn), single-threaded BLAS"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def metric_name():
+    return "batched S-matrix solves/s (FP64 varRCWA forward, per-order T/R)"
+
+
+def workload_config(a, batch):
+    n = 242 if a.workload == "c2" else None
+    return {"workload": ("config-2 pillar cells (11x11 orders, n=242, 256x256 raster)" if a.workload == "c2" else
+                         "config-3 uneven pillar batch (7..15 orders, n=98..450)"),
+            "batch_per_gpu": batch, "n": n, "pe": a.pe, "raster": f"{a.npix}x{a.npix}",
+            "integrator": "adaptive varRCWA (trisection), Redheffer star products",
+            "output": "per-order R/T, 2 polarisations, incidence from the superstrate",
+            "l2": "per-step working set (GBs of matrices) exceeds the 126 MB L2; no flush needed"}
+
+
+# ---------------------------------------------------------------------------
+# Our arm
+# ---------------------------------------------------------------------------
+def run_ours(a, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from varrcwa_b200.capi import Context
+
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    ctx = Context(dev)
+    descs = make_cells(a.workload, a.batch, rank, a.npix)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    fp64_peak = dgemm_peak_tflops(dev) if rank == 0 else None
+    for _ in range(a.warmup):
+        ctx.order_powers(descs, method="redheffer", pe=a.pe, side=1)
+    ctx.set_profiling(True)
+    clocks = ClockSampler(dev)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    dev_ms = 0.0
+    launches = 0
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        out = ctx.order_powers(descs, method="redheffer", pe=a.pe, side=1)
+        t = ctx.timing()
+        dev_ms += t["device_ms"]
+        launches += t["launches"]
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    barrier()
+    clk = clocks.stop()
+    stats = ctx.kernel_stats()
+    ctx.set_profiling(False)
+    statuses = [o["status"] for o in out]
+    # max over ranks
+    if world > 1:
+        tt = torch.tensor([dev_ms, wall], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dev_ms, wall = float(tt[0]), float(tt[1])
+    if rank != 0:
+        return
+    cells = a.batch * world * a.steps
+    value = cells / (dev_ms * 1e-3)
+    e2e = cells / wall
+    m = 121 if a.workload == "c2" else None
+    h2d = sum(len(np.asarray(d.get("eps", [])).tobytes()) for d in descs) + 256 * len(descs)
+    d2h = sum(2 * 2 * d["nx"] * d["ny"] * 8 for d in descs)
+    # dominant kernel family and its roofline
+    fam = max(stats.items(), key=lambda kv: kv[1]["ms"])
+    hbm_peak, hbm_src = measured_peaks()
+    name, f = fam
+    if f["flops"] > 0 and name in ("zgemm", "zinv", "hessenberg", "schur_qr", "trevc"):
+        achieved = f["flops"] / (f["ms"] * 1e-3) / 1e12
+        roof = {"kernel": name, "bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp64_peak if fp64_peak else None,
+                "peak_source": "measured cuBLAS DGEMM (FP64 DMMA) on this GPU, 8192^3",
+                "avg_launch_ms": f["ms"] / max(f["launches"], 1), "traffic": None}
+    else:
+        achieved = f["bytes"] / (f["ms"] * 1e-3) / 1e9
+        roof = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak, "peak_source": f"{hbm_src} MEASURED_PEAKS.json hbm_gbs",
+                "avg_launch_ms": f["ms"] / max(f["launches"], 1), "traffic": None}
+    gemm = stats.get("zgemm")
+    breakdown = {k: {"ms": round(v["ms"], 3), "share": round(v["ms"] / sum(x["ms"] for x in stats.values()), 4),
+                     "launches": v["launches"],
+                     "tflops": round(v["flops"] / (v["ms"] * 1e-3) / 1e12, 3) if v["flops"] and v["ms"] else None}
+                 for k, v in sorted(stats.items(), key=lambda kv: -kv[1]["ms"])}
+    line = {
+        "metric": metric_name(), "value": value, "unit": "solves/s", "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": dev_ms / a.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "complex128", "data": "synthetic",
+        "config": workload_config(a, a.batch), "parallelism": f"replicas x{world}",
+        "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches, "roofline": roof, "clocks": clk, "kernel_breakdown": breakdown,
+        "statuses_nonzero": int(sum(1 for s in statuses if s)),
+    }
+    if gemm:
+        line["zgemm_tflops"] = gemm["flops"] / (gemm["ms"] * 1e-3) / 1e12
+        line["fp64_dgemm_peak_tflops"] = fp64_peak
+    if world == 1 and not a.no_cpu_baseline:
+        sample = descs[: a.cpu_cells]
+        dt = cpu_sample(sample, a.pe)
+        line["cpu_baseline"] = {"value": len(sample) / dt, "unit": "solves/s", "cores": os.cpu_count(),
+                                "kind": "port",
+                                "sample": f"{len(sample)} cell(s) of the same workload through the numpy oracle "
+                                          f"(OpenBLAS threads = host cores), {dt:.1f} s"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        run_reference(a, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        run_ours(a, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

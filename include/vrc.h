@@ -183,6 +183,20 @@ int vrc_differential(vrc_context* ctx, int ncells, const vrc_cell* cells, int N,
 int vrc_order_powers(vrc_context* ctx, int ncells, const vrc_cell* cells, int method, double pe, int max_depth,
                      int nslices, int side, int flux_norm, double* R, double* T, int* status);
 
+/* ---- instrumentation (no counterpart in the reference) ---------------------
+ * Per-kernel-family device time measured with CUDA events on the engine
+ * stream, with the algorithmic FP64 flops and bytes of the timed launches. */
+typedef struct {
+  char name[32];
+  double ms;
+  long long launches;
+  double flops;
+  double bytes;
+} vrc_kernel_stat;
+int vrc_set_profiling(vrc_context* ctx, int enable); /* also resets the counters */
+/* Returns the number of families (fills at most max entries of out). */
+int vrc_get_kernel_stats(vrc_context* ctx, int max, vrc_kernel_stat* out);
+
 /* ---- batched kernels (host buffers) --------------------------------------- */
 /* C[b] = A[b] * B[b]  (batch n*n complex GEMMs on FP64 tensor cores). */
 int vrc_zgemm(vrc_context* ctx, int batch, int n, const vrc_complex* A, const vrc_complex* B, vrc_complex* C);

@@ -22,7 +22,8 @@ GEOM_GRID, GEOM_PILLAR, GEOM_PIXELS = 0, 1, 2
 EXPORTS = [
     "vrc_create", "vrc_destroy", "vrc_last_error", "vrc_status_string", "vrc_get_timing", "vrc_sample_pq",
     "vrc_wave_solve", "vrc_eig", "vrc_redheffer", "vrc_redheffer_segments", "vrc_get_tree", "vrc_rcwa",
-    "vrc_differential", "vrc_order_powers", "vrc_zgemm", "vrc_zinv",
+    "vrc_differential", "vrc_order_powers", "vrc_zgemm", "vrc_zinv", "vrc_set_profiling",
+    "vrc_get_kernel_stats",
 ]
 
 
@@ -66,6 +67,11 @@ class VrcTiming(C.Structure):
     _fields_ = [("device_ms", C.c_double), ("launches", C.c_longlong)]
 
 
+class VrcKernelStat(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("ms", C.c_double), ("launches", C.c_longlong), ("flops", C.c_double),
+                ("bytes", C.c_double)]
+
+
 class VrcError(RuntimeError):
     def __init__(self, status: int, msg: str):
         super().__init__(f"vrc status {status}: {msg}")
@@ -106,6 +112,8 @@ def lib():
                                    C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int)]
     L.vrc_zgemm.argtypes = [vp, C.c_int, C.c_int, CP, CP, CP]
     L.vrc_zinv.argtypes = [vp, C.c_int, C.c_int, CP, C.POINTER(C.c_int)]
+    L.vrc_set_profiling.argtypes = [vp, C.c_int]
+    L.vrc_get_kernel_stats.argtypes = [vp, C.c_int, C.POINTER(VrcKernelStat)]
     _lib = L
     return L
 
@@ -214,6 +222,18 @@ class Context:
         t = VrcTiming()
         self._check(self.L.vrc_get_timing(self.h, C.byref(t)))
         return {"device_ms": t.device_ms, "launches": int(t.launches)}
+
+    def set_profiling(self, on: bool = True):
+        self._check(self.L.vrc_set_profiling(self.h, 1 if on else 0))
+
+    def kernel_stats(self) -> Dict[str, dict]:
+        cnt = self.L.vrc_get_kernel_stats(self.h, 0, None)
+        if cnt < 0:
+            raise VrcError(-cnt, self.L.vrc_last_error(self.h).decode())
+        arr = (VrcKernelStat * max(cnt, 1))()
+        self.L.vrc_get_kernel_stats(self.h, cnt, arr)
+        return {arr[i].name.decode(): {"ms": arr[i].ms, "launches": int(arr[i].launches), "flops": arr[i].flops,
+                                       "bytes": arr[i].bytes} for i in range(cnt)}
 
     # ---- assembly / eigen ----
     def sample_pq(self, desc: dict, zs: Sequence[float]):

@@ -416,6 +416,34 @@ int vrc_order_powers(vrc_context* ctx, int ncells, const vrc_cell* cells, int me
   });
 }
 
+int vrc_set_profiling(vrc_context* ctx, int enable) {
+  return guarded(ctx, [&] {
+    ctx->eng->set_profiling(enable != 0);
+    ctx->eng->reset_fam_stats();
+  });
+}
+
+int vrc_get_kernel_stats(vrc_context* ctx, int max, vrc_kernel_stat* out) {
+  if (!ctx) return -VRC_EINVAL;
+  int count = 0;
+  int st = guarded(ctx, [&] {
+    auto& f = ctx->eng->fam_stats();
+    for (auto& kv : f) {
+      if (out && count < max) {
+        vrc_kernel_stat& o = out[count];
+        std::memset(o.name, 0, sizeof(o.name));
+        std::strncpy(o.name, kv.first.c_str(), sizeof(o.name) - 1);
+        o.ms = kv.second.ms;
+        o.launches = kv.second.launches;
+        o.flops = kv.second.flops;
+        o.bytes = kv.second.bytes;
+      }
+      ++count;
+    }
+  });
+  return st == VRC_OK ? count : -st;
+}
+
 int vrc_zgemm(vrc_context* ctx, int batch, int n, const vrc_complex* A, const vrc_complex* B, vrc_complex* C) {
   return guarded(ctx, [&] {
     if (batch < 0 || n < 1 || (batch > 0 && (!A || !B || !C))) throw vrc::StatusError(VRC_EINVAL, "invalid arguments");

@@ -602,9 +602,11 @@ void Engine::order_powers(const std::vector<CellSpec>& cells, const std::vector<
       }
       ab[b] = (double*)bytes(2 * m * sizeof(double));
     }
-    matvec_batched(upload(mv1), (int)mv1.size(), n, stream_);
-    matvec_batched(upload(mv2), (int)mv2.size(), n, stream_);
-    launches += 2;
+    {
+      Prof pr(*this, "powers", 16.0 * n * (double)n * (mv1.size() + mv2.size()), 16.0 * n * (double)n * (mv1.size() + mv2.size()), 2);
+      matvec_batched(upload(mv1), (int)mv1.size(), n, stream_);
+      matvec_batched(upload(mv2), (int)mv2.size(), n, stream_);
+    }
     std::vector<PowerDesc> pd;
     std::vector<std::vector<double>> hab(B);
     for (size_t b = 0; b < B; ++b) {
@@ -629,8 +631,10 @@ void Engine::order_powers(const std::vector<CellSpec>& cells, const std::vector<
         pd.push_back({rf[k], tf[k], ab[b], ab[b] + m, Rd[k], Td[k], ein, eout, s.k0(), tn});
       }
     }
-    order_power_batched(upload(pd), (int)pd.size(), m, stream_);
-    ++launches;
+    {
+      Prof pr(*this, "powers", 0.0, 64.0 * m * (double)pd.size());
+      order_power_batched(upload(pd), (int)pd.size(), m, stream_);
+    }
     for (size_t b = 0; b < B; ++b) {
       Rout[ids[b]].resize(2 * m);
       Tout[ids[b]].resize(2 * m);

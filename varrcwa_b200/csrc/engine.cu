@@ -92,6 +92,11 @@ Engine::~Engine() {
   cudaSetDevice(device_);
   cudaStreamSynchronize(stream_);
   pools_.clear();
+  for (auto& p : pend_prof_) {
+    cudaEventDestroy(p.a);
+    cudaEventDestroy(p.b);
+  }
+  for (auto e : ev_pool_) cudaEventDestroy(e);
   if (ws_) cudaFree(ws_);
   if (d_stage_) cudaFree(d_stage_);
   if (h_stage_) cudaFreeHost(h_stage_);
@@ -101,6 +106,62 @@ Engine::~Engine() {
 void Engine::sync() {
   VRC_CUDA_CHECK(cudaStreamSynchronize(stream_));
   stage_off_ = 0;
+  if (!pend_prof_.empty()) resolve_prof();
+}
+
+cudaEvent_t Engine::take_event() {
+  if (ev_pool_.empty()) {
+    cudaEvent_t e;
+    VRC_CUDA_CHECK(cudaEventCreate(&e));
+    return e;
+  }
+  cudaEvent_t e = ev_pool_.back();
+  ev_pool_.pop_back();
+  return e;
+}
+
+void Engine::resolve_prof() {
+  for (auto& p : pend_prof_) {
+    float ms = 0.f;
+    VRC_CUDA_CHECK(cudaEventElapsedTime(&ms, p.a, p.b));
+    FamStat& f = fam_[p.fam];
+    f.ms += ms;
+    f.launches += p.nl;
+    f.flops += p.flops;
+    f.bytes += p.bytes;
+    ev_pool_.push_back(p.a);
+    ev_pool_.push_back(p.b);
+  }
+  pend_prof_.clear();
+}
+
+void Engine::set_profiling(bool on) {
+  sync();
+  profiling_ = on;
+}
+std::map<std::string, Engine::FamStat>& Engine::fam_stats() {
+  sync();
+  return fam_;
+}
+void Engine::reset_fam_stats() {
+  sync();
+  fam_.clear();
+}
+
+Engine::Prof::Prof(Engine& eng, const char* f, double fl, double by, int nlaunch)
+    : e(eng), fam(f), flops(fl), bytes(by), nl(nlaunch) {
+  if (e.profiling_) {
+    a = e.take_event();
+    VRC_CUDA_CHECK(cudaEventRecord(a, e.stream_));
+  }
+}
+Engine::Prof::~Prof() {
+  e.launches += nl;
+  if (a) {
+    cudaEvent_t b = e.take_event();
+    cudaEventRecord(b, e.stream_);
+    e.pend_prof_.push_back({fam, a, b, flops, bytes, nl});
+  }
 }
 
 BlockPool& Engine::pool(size_t bytes) {
@@ -168,8 +229,9 @@ void Engine::gemm(std::vector<GemmDesc>& d, int n, cplx alpha, cplx beta, double
   for (size_t b0 = 0; b0 < d.size(); b0 += per) {
     size_t nb = std::min(per, d.size() - b0);
     GemmDesc* dd = upload(d.data() + b0, nb);
+    const double nn3 = (double)n * n * n;
+    Prof pr(*this, "zgemm", 8.0 * nn3 * nb, 48.0 * n * (double)n * nb);
     zgemm_batched(dd, (int)nb, n, alpha, beta, delta, stream_);
-    ++launches;
   }
 }
 
@@ -181,8 +243,11 @@ void Engine::inverse(const std::vector<cplx*>& mats, int n, std::vector<int>* st
     dst = (int*)bytes(mats.size() * sizeof(int));
     VRC_CUDA_CHECK(cudaMemsetAsync(dst, 0, mats.size() * sizeof(int), stream_));
   }
-  zinv_batched(dm, (int)mats.size(), n, dst, stream_);
-  ++launches;
+  {
+    const double nn3 = (double)n * n * n;
+    Prof pr(*this, "zinv", 8.0 * nn3 * mats.size(), 32.0 * n * (double)n * mats.size());
+    zinv_batched(dm, (int)mats.size(), n, dst, stream_);
+  }
   if (status) {
     std::vector<int> h(mats.size());
     VRC_CUDA_CHECK(cudaMemcpyAsync(h.data(), dst, h.size() * sizeof(int), cudaMemcpyDeviceToHost, stream_));
@@ -208,8 +273,8 @@ void Engine::axpby(const std::vector<const cplx*>& A, const std::vector<const cp
     const cplx* const* da = upload(A.data() + b0, nb);
     const cplx* const* db = upload(B.data() + b0, nb);
     cplx* const* dc = upload(C.data() + b0, nb);
+    Prof pr(*this, "elementwise", 0.0, 48.0 * n * (double)n * nb);
     axpby_batched(da, db, dc, alpha, beta, delta, (int)nb, n, stream_);
-    ++launches;
   }
 }
 
@@ -504,11 +569,17 @@ void Engine::assemble(std::vector<SampleReq>& reqs, std::vector<int>* status) {
         for (size_t b = 0; b < B; ++b) v[b] = ws + b * per + off;
         return v;
       };
+      // Fourier/Toeplitz stage (A1-A4) timed as one family; algorithmic
+      // bytes: eps raster in, fe11/fe22/fe33 out.
+      const double asm_flops =
+          8.0 * B * ((double)P * nr * nc * 2 + (double)Q * nc * nr + (double)P * Q * nr + (double)nx * nx * Q * nr +
+                     (double)P * ny * ny * nc + (double)nr * nx * nx * nx + (double)nc * ny * ny * ny);
+      const double asm_bytes = 16.0 * B * ((double)nr * nc + 3.0 * m * m);
+      std::unique_ptr<Prof> asm_prof(new Prof(*this, "assembly", asm_flops, asm_bytes, 12 + (k.pillar ? 1 : 0)));
       if (k.pillar) {
         const CellSpec& s0 = *reqs[idx[c0]].spec;
         double* drad = upload(radius);
         pillar_raster(drad, upload(epsw), (int)B, s0.npx, s0.npy, s0.Lx, s0.Ly, s0.eps_in, s0.eps_out, stream_);
-        ++launches;
         // pillar cells of one group may differ in eps_in/eps_out: rasterise per
         // distinct material pair
         for (size_t b = 1; b < B; ++b) {
@@ -517,7 +588,7 @@ void Engine::assemble(std::vector<SampleReq>& reqs, std::vector<int>* status) {
               sb.eps_out.y != s0.eps_out.y || sb.Lx != s0.Lx || sb.Ly != s0.Ly) {
             std::vector<cplx*> one = {epsw[b]};
             pillar_raster(drad + b, upload(one), 1, sb.npx, sb.npy, sb.Lx, sb.Ly, sb.eps_in, sb.eps_out, stream_);
-            ++launches;
+            ++launches;  // extra raster for a different material pair
           }
         }
       }
@@ -530,7 +601,6 @@ void Engine::assemble(std::vector<SampleReq>& reqs, std::vector<int>* status) {
       std::vector<cplx*> invv(B);
       for (size_t b = 0; b < B; ++b) invv[b] = const_cast<cplx*>(invp[b]);
       reciprocal(upload(epsmut), upload(invv), (int)B, nr * nc, stream_);
-      launches += 4;
       auto cst = [](const std::vector<cplx*>& v) { return std::vector<const cplx*>(v.begin(), v.end()); };
       auto ax = ptrs(o_ax), bx = ptrs(o_bx), ay = ptrs(o_ay), f2 = ptrs(o_f2);
       // AX = Ex * inv_cm (nc x nr), BX = Ex * eps_cm
@@ -540,7 +610,6 @@ void Engine::assemble(std::vector<SampleReq>& reqs, std::vector<int>* status) {
       small_gemm(Q, nc, nr, upload(cst(ey)), Q, upload(cst(invv)), nc, 1, upload(ay), Q, (int)B, stream_);
       // F2 = BX * Ey^T (P x Q)
       small_gemm(P, Q, nr, upload(cst(bx)), P, upload(cst(ey)), Q, 1, upload(f2), P, (int)B, stream_);
-      launches += 4;
       auto ti = ptrs(o_ti), tj = ptrs(o_tj);
       int* dstat = nullptr;
       if (status) {
@@ -549,16 +618,14 @@ void Engine::assemble(std::vector<SampleReq>& reqs, std::vector<int>* status) {
       }
       toeplitz_inverses(upload(cst(ax)), upload(ti), nx, nr, (int)B, dstat, stream_);
       toeplitz_inverses(upload(cst(ay)), upload(tj), ny, nc, (int)B, dstat, stream_);
-      launches += 2;
       auto g11 = ptrs(o_g11), g22 = ptrs(o_g22);
       small_gemm(nx * nx, Q, nr, upload(cst(ti)), nx * nx, upload(cst(ey)), Q, 1, upload(g11), nx * nx, (int)B,
                  stream_);
       small_gemm(P, ny * ny, nc, upload(cst(exs)), P, upload(cst(tj)), ny * ny, 1, upload(g22), P, (int)B, stream_);
-      launches += 2;
       auto fe11 = ptrs(o_fe11), fe22 = ptrs(o_fe22), fe33 = ptrs(o_fe33);
       gather_fe(upload(cst(g11)), upload(cst(g22)), upload(cst(f2)), upload(fe11), upload(fe22), upload(fe33), nx,
                 ny, (int)B, stream_);
-      ++launches;
+      asm_prof.reset();
       // fe33^{-1} (BDCSVD solve of the square system, Layer.cpp:84-86)
       std::vector<int> inv_status;
       inverse(fe33, m, status ? &inv_status : nullptr);
@@ -588,9 +655,9 @@ void Engine::assemble(std::vector<SampleReq>& reqs, std::vector<int>* status) {
           std::vector<const cplx*> f1(fe11.begin() + b, fe11.begin() + e);
           std::vector<const cplx*> f2v(fe22.begin() + b, fe22.begin() + e);
           std::vector<cplx*> pv(Pp.begin() + b, Pp.begin() + e), qv(Qp.begin() + b, Qp.begin() + e);
+          Prof pr(*this, "assembly", 0.0, 16.0 * (e - b) * (3.0 * m * m + 8.0 * m * m));
           assemble_periodic(upload(fi), upload(f1), upload(f2v), dab + b * 2 * m, dab + b * 2 * m + m, dk + b,
                             upload(pv), upload(qv), m, (int)(e - b), stream_);
-          ++launches;
           b = e - 1;
         }
       } else {
@@ -619,10 +686,10 @@ void Engine::assemble(std::vector<SampleReq>& reqs, std::vector<int>* status) {
           const CellDev* cd = reqs[idx[c0 + b]].cd;
           auto sl = [&](const std::vector<cplx*>& v) { return std::vector<const cplx*>(v.begin() + b, v.begin() + e); };
           std::vector<cplx*> pv(Pp.begin() + b, Pp.begin() + e), qv(Qp.begin() + b, Qp.begin() + e);
+          Prof pr(*this, "assembly", 0.0, 16.0 * (e - b) * (6.0 * m * m + 8.0 * m * m));
           assemble_dense(upload(sl(KxF2h)), upload(sl(KxF1h)), upload(sl(KyF2h)), upload(sl(KyF1h)), upload(sl(fe11)),
                          upload(sl(fe22)), cd->KxKy, cd->KxKx, cd->KyKy, cd->KyKx, dk + b, upload(pv), upload(qv), m,
                          (int)(e - b), stream_);
-          ++launches;
           b = e - 1;
         }
       }
@@ -671,19 +738,32 @@ void Engine::eig(std::vector<EigReq>& reqs, int n, std::vector<int>* status) {
       g.push_back({r.P, r.Q, H[b], nullptr, nullptr, nullptr});
     }
     gemm(g, n, mk(1, 0), mk(0, 0), 0.0);  // PQ = P*Q
-    hessenberg_batched(upload(H), upload(Z), (int)B, n, stream_);
+    // nominal LAPACK counts (real flops): zgehrd 40/3 n^3 + zunghr 16/3 n^3,
+    // complex Schur with Z ~ 80 n^3, ztrevc 4/3 n^3
+    const double nn3 = (double)n * n * n, mbytes = 16.0 * n * (double)n;
+    {
+      Prof pr(*this, "hessenberg", (56.0 / 3.0) * nn3 * B, 3.0 * mbytes * B);
+      hessenberg_batched(upload(H), upload(Z), (int)B, n, stream_);
+    }
     int* dstat = (int*)bytes(B * sizeof(int));
     VRC_CUDA_CHECK(cudaMemsetAsync(dstat, 0, B * sizeof(int), stream_));
-    schur_batched(upload(H), upload(Z), upload(lam), (int)B, n, dstat, stream_);
-    trevc_batched(upload(H), upload(Y), (int)B, n, stream_);
-    launches += 3;
+    {
+      Prof pr(*this, "schur_qr", 80.0 * nn3 * B, 4.0 * mbytes * B);
+      schur_batched(upload(H), upload(Z), upload(lam), (int)B, n, dstat, stream_);
+    }
+    {
+      Prof pr(*this, "trevc", (4.0 / 3.0) * nn3 * B, 1.5 * mbytes * B);
+      trevc_batched(upload(H), upload(Y), (int)B, n, stream_);
+    }
     g.clear();
     for (size_t b = 0; b < B; ++b) g.push_back({Z[b], Y[b], W[b], nullptr, nullptr, nullptr});
     gemm(g, n, mk(1, 0), mk(0, 0), 0.0);  // X = Z Y
-    vecnorm_batched(upload(W), (int)B, n, stream_);
-    std::vector<const cplx*> lamc(lam.begin(), lam.end());
-    gamma_batched(upload(lamc), upload(gam), upload(ig), (int)B, n, stream_);
-    launches += 2;
+    {
+      Prof pr(*this, "elementwise", 0.0, 2.0 * mbytes * B, 2);
+      vecnorm_batched(upload(W), (int)B, n, stream_);
+      std::vector<const cplx*> lamc(lam.begin(), lam.end());
+      gamma_batched(upload(lamc), upload(gam), upload(ig), (int)B, n, stream_);
+    }
     g.clear();
     for (size_t b = 0; b < B; ++b) g.push_back({reqs[c0 + b].Q, W[b], V[b], nullptr, nullptr, ig[b]});
     gemm(g, n, mk(1, 0), mk(0, 0), 0.0);  // V = Q W diag(1/gamma)
@@ -756,8 +836,10 @@ void Engine::segments(std::vector<SegReq>& reqs, int n) {
         g1.push_back({D[b], pq == 0 ? s.V : s.W, T[b], nullptr, nullptr, nullptr});
         g2.push_back({pq == 0 ? s.Winv : s.Vinv, T[b], out, nullptr, nullptr, nullptr});
       }
-      sub_batched(upload(a), upload(r), upload(D), (int)B, (long long)nn, stream_);
-      ++launches;
+      {
+        Prof pr(*this, "elementwise", 0.0, 48.0 * nn * B);
+        sub_batched(upload(a), upload(r), upload(D), (int)B, (long long)nn, stream_);
+      }
       gemm(g1, n, mk(1, 0), mk(0, 0), 0.0);
       gemm(g2, n, mk(1, 0), mk(0, 0), 0.0);
     };
@@ -770,8 +852,10 @@ void Engine::segments(std::vector<SegReq>& reqs, int n) {
       const SegReq& s = reqs[c0 + b];
       sd[b] = {X0[b], Y0[b], X2[b], Y2[b], s.gam, s.tdd, s.tuu, s.rud, s.rdu, s.err, s.z0, s.z1, s.k0};
     }
-    simpson_batched(upload(sd), (int)B, n, stream_);
-    ++launches;
+    {
+      Prof pr(*this, "simpson", 0.0, 16.0 * 8.0 * nn * B);
+      simpson_batched(upload(sd), (int)B, n, stream_);
+    }
   }
 }
 
@@ -805,8 +889,10 @@ void Engine::project_left(std::vector<ProjReq>& reqs, int n, std::vector<int>* s
       g.push_back({r.Vinv, r.leftV, Bm[b], nullptr, nullptr, nullptr});
     }
     gemm(g, n, mk(1, 0), mk(0, 0), 0.0);
-    ab_batched(upload(A), upload(Bm), (int)B, (long long)nn, stream_);
-    ++launches;
+    {
+      Prof pr(*this, "elementwise", 0.0, 64.0 * nn * B);
+      ab_batched(upload(A), upload(Bm), (int)B, (long long)nn, stream_);
+    }
     g.clear();
     for (size_t b = 0; b < B; ++b) g.push_back({reqs[c0 + b].rdu, Bm[b], M[b], A[b], nullptr, nullptr});
     gemm(g, n, mk(-1, 0), mk(1, 0), 0.0);  // M = A - rdu B
@@ -872,8 +958,10 @@ void Engine::project_right(std::vector<ProjRReq>& reqs, int n, std::vector<int>*
       g.push_back({r.leftVinv, r.V1, Bm[b], nullptr, nullptr, nullptr});
     }
     gemm(g, n, mk(1, 0), mk(0, 0), 0.0);
-    ab_batched(upload(A), upload(Bm), (int)B, (long long)nn, stream_);
-    ++launches;
+    {
+      Prof pr(*this, "elementwise", 0.0, 64.0 * nn * B);
+      ab_batched(upload(A), upload(Bm), (int)B, (long long)nn, stream_);
+    }
     g.clear();
     for (size_t b = 0; b < B; ++b) g.push_back({reqs[c0 + b].Rud, Bm[b], M[b], A[b], nullptr, nullptr});
     gemm(g, n, mk(-1, 0), mk(1, 0), 0.0);  // M = A - Rud B
@@ -1056,8 +1144,10 @@ void Engine::rcwa_slabs(std::vector<SlabReq>& reqs, int n, std::vector<int>* sta
     }
     gemm(g, n, mk(1, 0), mk(0, 0), 0.0);
     // A, B = (F0 +- G0)/2; the common factor 1/2 is exact and cancels
-    ab_batched(upload(A), upload(Bm), (int)B, (long long)nn, stream_);
-    ++launches;
+    {
+      Prof pr(*this, "elementwise", 0.0, 64.0 * nn * B);
+      ab_batched(upload(A), upload(Bm), (int)B, (long long)nn, stream_);
+    }
     copy(A, Ai, n);
     std::vector<int> ist;
     inverse(Ai, n, status ? &ist : nullptr);
@@ -1065,9 +1155,11 @@ void Engine::rcwa_slabs(std::vector<SlabReq>& reqs, int n, std::vector<int>* sta
     for (size_t b = 0; b < B; ++b) ts[b] = reqs[c0 + b].dz / reqs[c0 + b].k0;
     double* dts = upload(ts);
     std::vector<const cplx*> Ac(A.begin(), A.end()), Bc(Bm.begin(), Bm.end()), gc(gam.begin(), gam.end());
-    phase_rows_batched(upload(Ac), upload(gc), dts, upload(XA), (int)B, n, stream_);
-    phase_rows_batched(upload(Bc), upload(gc), dts, upload(XB), (int)B, n, stream_);
-    launches += 2;
+    {
+      Prof pr(*this, "elementwise", 0.0, 64.0 * nn * B, 2);
+      phase_rows_batched(upload(Ac), upload(gc), dts, upload(XA), (int)B, n, stream_);
+      phase_rows_batched(upload(Bc), upload(gc), dts, upload(XB), (int)B, n, stream_);
+    }
     g.clear();
     for (size_t b = 0; b < B; ++b) {
       g.push_back({Ai[b], Bm[b], iAB[b], nullptr, nullptr, nullptr});
@@ -1187,9 +1279,11 @@ void Engine::diff_slices(std::vector<DiffReq>& reqs, int n, std::vector<int>* st
     }
     gemm(g, n, mk(1, 0), mk(0, 0), 0.0);
     // A11 = (U1+U3)/2, A21 = (U1-U3)/2, A12 = (U2+U4)/2, A22 = (U2-U4)/2
-    ab_batched(upload(U1), upload(U3), (int)B, (long long)nn, stream_);
-    ab_batched(upload(U2), upload(U4), (int)B, (long long)nn, stream_);
-    launches += 2;
+    {
+      Prof pr(*this, "elementwise", 0.0, 128.0 * nn * B, 2);
+      ab_batched(upload(U1), upload(U3), (int)B, (long long)nn, stream_);
+      ab_batched(upload(U2), upload(U4), (int)B, (long long)nn, stream_);
+    }
     g.clear();
     for (size_t b = 0; b < B; ++b) {
       const DiffReq& r = reqs[c0 + b];

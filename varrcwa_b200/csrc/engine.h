@@ -5,6 +5,7 @@
 #include <functional>
 #include <map>
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "common.cuh"
@@ -237,6 +238,28 @@ class Engine {
   // counters
   long long launches = 0;
 
+  // Per-kernel-family timing with CUDA events on the engine stream
+  // (enabled on demand; resolved at every sync()).
+  struct FamStat {
+    double ms = 0.0;
+    long long launches = 0;
+    double flops = 0.0;  // algorithmic real FP64 flops
+    double bytes = 0.0;  // algorithmic bytes moved
+  };
+  void set_profiling(bool on);
+  bool profiling() const { return profiling_; }
+  std::map<std::string, FamStat>& fam_stats();
+  void reset_fam_stats();
+  struct Prof {
+    Engine& e;
+    const char* fam;
+    double flops, bytes;
+    int nl;
+    cudaEvent_t a = nullptr;
+    Prof(Engine& eng, const char* f, double fl = 0.0, double by = 0.0, int nlaunch = 1);
+    ~Prof();
+  };
+
  private:
   int device_;
   cudaStream_t stream_;
@@ -247,6 +270,18 @@ class Engine {
   size_t stage_cap_ = 0, stage_off_ = 0;
   void* ws_ = nullptr;
   size_t ws_cap_ = 0;
+  bool profiling_ = false;
+  struct PendingProf {
+    const char* fam;
+    cudaEvent_t a, b;
+    double flops, bytes;
+    int nl;
+  };
+  std::vector<PendingProf> pend_prof_;
+  std::vector<cudaEvent_t> ev_pool_;
+  std::map<std::string, FamStat> fam_;
+  cudaEvent_t take_event();
+  void resolve_prof();
   BlockPool& pool(size_t bytes);
   void* stage(const void* data, size_t bytes);
   struct EndBasis {
