@@ -203,6 +203,24 @@ int vrc_zgemm(vrc_context* ctx, int batch, int n, const vrc_complex* A, const vr
 /* In-place inverse of batch n*n matrices; status[b] = VRC_ESINGULAR on a zero pivot. */
 int vrc_zinv(vrc_context* ctx, int batch, int n, vrc_complex* A, int* status);
 
+/* ---- eigen-decomposition without device allocation ------------------------
+ * No counterpart in the reference.  For callers that cannot let a library
+ * call cudaMalloc (applications that own all device memory through their
+ * own pool, pipelines where an allocation's implicit device synchronisation
+ * is not acceptable).  Same kernels as vrc_eig for ONE n x n matrix:
+ * A (input, not modified), W (eigenvectors, unit 2-norm, largest component
+ * real) and lam (eigenvalues) are DEVICE pointers, column-major complex128,
+ * on the calling thread's current device; work is queued on `stream`
+ * (a cudaStream_t, NULL = legacy default stream) and the call returns after
+ * the stream has drained.  Scratch is a fixed area inside the library
+ * (about 3 MiB per device, held until exit), so n must be in
+ * [2, VRC_EIG_NOALLOC_MAX_N]; larger n returns VRC_EINVAL.  All calls share
+ * that area: calls that overlap on the GPU race and must be serialised by
+ * the caller.  The first call on a device looks the area up; make it before
+ * any stream capture.  Returns VRC_ENOCONV if the QR iteration hit its cap. */
+#define VRC_EIG_NOALLOC_MAX_N 256
+int vrc_eig_noalloc(int n, const vrc_complex* A, vrc_complex* W, vrc_complex* lam, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -20,7 +20,7 @@ BUILD = ROOT / "_build"
 LIB = PKG / "libvrc.so"
 
 SOURCES = ["gemm.cu", "inverse.cu", "eig.cu", "assembly.cu", "segment.cu", "engine.cu", "drivers.cu",
-           "capi.cu"]
+           "capi.cu", "noalloc.cu"]
 HEADERS = ["common.cuh", "kernels.h", "engine.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",

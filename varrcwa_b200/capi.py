@@ -23,7 +23,7 @@ EXPORTS = [
     "vrc_create", "vrc_destroy", "vrc_last_error", "vrc_status_string", "vrc_get_timing", "vrc_sample_pq",
     "vrc_wave_solve", "vrc_eig", "vrc_redheffer", "vrc_redheffer_segments", "vrc_get_tree", "vrc_rcwa",
     "vrc_differential", "vrc_order_powers", "vrc_zgemm", "vrc_zinv", "vrc_set_profiling",
-    "vrc_get_kernel_stats",
+    "vrc_get_kernel_stats", "vrc_eig_noalloc",
 ]
 
 
@@ -114,6 +114,7 @@ def lib():
     L.vrc_zinv.argtypes = [vp, C.c_int, C.c_int, CP, C.POINTER(C.c_int)]
     L.vrc_set_profiling.argtypes = [vp, C.c_int]
     L.vrc_get_kernel_stats.argtypes = [vp, C.c_int, C.POINTER(VrcKernelStat)]
+    L.vrc_eig_noalloc.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     _lib = L
     return L
 
