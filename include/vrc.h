@@ -213,7 +213,7 @@ int vrc_zinv(vrc_context* ctx, int batch, int n, vrc_complex* A, int* status);
  * on the calling thread's current device; work is queued on `stream`
  * (a cudaStream_t, NULL = legacy default stream) and the call returns after
  * the stream has drained.  Scratch is a fixed area inside the library
- * (about 3 MiB per device, held until exit), so n must be in
+ * (about 22 MiB per device, held until exit), so n must be in
  * [2, VRC_EIG_NOALLOC_MAX_N]; larger n returns VRC_EINVAL.  All calls share
  * that area: calls that overlap on the GPU race and must be serialised by
  * the caller.  The first call on a device looks the area up; make it before

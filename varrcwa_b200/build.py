@@ -19,9 +19,9 @@ CSRC = PKG / "csrc"
 BUILD = ROOT / "_build"
 LIB = PKG / "libvrc.so"
 
-SOURCES = ["gemm.cu", "inverse.cu", "eig.cu", "assembly.cu", "segment.cu", "engine.cu", "drivers.cu",
+SOURCES = ["gemm.cu", "inverse.cu", "eig.cu", "qr.cu", "assembly.cu", "segment.cu", "engine.cu", "drivers.cu",
            "capi.cu", "noalloc.cu"]
-HEADERS = ["common.cuh", "kernels.h", "engine.h"]
+HEADERS = ["common.cuh", "kernels.h", "engine.h", "householder.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
          "-Xcompiler", "-Wno-unused-function", "--expt-relaxed-constexpr"]

@@ -6,22 +6,15 @@
 //                    (H = Q^H A Q) with the left and right reflector
 //                    applications fused into one rank-2 update per column,
 //                    then backward accumulation of Q.
-//   2. hqr_kernel    complex Schur form T = Z^H A Z by implicitly shifted
-//                    single-shift QR (Wilkinson shifts, exceptional shifts at
-//                    iterations 10/20, deflation on small subdiagonals).  The
-//                    bulge chase runs in chunks of B steps: one warp chases
-//                    the bulge through a (B+3)^2 diagonal window held in
-//                    shared memory; the chunk's B rotations are then applied
-//                    by the whole CTA to the rows/columns outside the window
-//                    and to Z, each thread streaming one row or column.
+//   2. hqr_kernel    complex Schur form T = Z^H A Z (qr.cu: multi-bulge
+//                    shifted QR with a rotation log replayed onto Z).
 //   3. trevc_kernel  eigenvectors of T by back substitution (one warp per
 //                    eigenvalue, near-singular diagonals perturbed to smin).
 //   4. vecnorm_kernel  X = Z Y is formed by the GEMM; each column is scaled to
 //                    unit 2-norm with its largest component real (the zgeev
 //                    convention).
-// Every loop is bounded: QR gives up after 30*max(10,n) iterations per
-// eigenvalue and reports ST_ENOCONV through the status array.
 #include "common.cuh"
+#include "householder.cuh"
 #include "kernels.h"
 
 namespace vrc {
@@ -42,24 +35,6 @@ __device__ __forceinline__ double warp_sumd(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
-}
-
-// Elementary reflector for a vector (alpha, x): returns beta (real), tau and
-// the scale applied to x so that v = (1, x*scale).  Published Householder
-// construction (Golub & Van Loan 5.1.13, complex form).
-__device__ __forceinline__ void householder(cplx alpha, double xnorm2, double* beta, cplx* tau,
-                                            cplx* scale) {
-  if (xnorm2 == 0.0 && alpha.y == 0.0) {
-    *beta = alpha.x;
-    *tau = mk(0.0, 0.0);
-    *scale = mk(0.0, 0.0);
-    return;
-  }
-  double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xnorm2);
-  double b = alpha.x >= 0.0 ? -nrm : nrm;
-  *beta = b;
-  *tau = mk((b - alpha.x) / b, -alpha.y / b);
-  *scale = cinv(mk(alpha.x - b, alpha.y));
 }
 
 // ---------------------------------------------------------------------------
@@ -218,249 +193,8 @@ __global__ void __launch_bounds__(HESS_THREADS)
   }
 }
 
-// ---------------------------------------------------------------------------
-// 2. Shifted QR to complex Schur form
-// ---------------------------------------------------------------------------
-constexpr int QR_THREADS = 256;
-constexpr int QB = 32;          // bulge-chase steps per chunk
-constexpr int QD = QB + 3;      // diagonal window size
-constexpr double ULP = 2.220446049250313e-16;  // 2^-52 (unit roundoff * base)
-constexpr double SMLNUM_BASE = 2.2250738585072014e-308;
-
-__device__ __forceinline__ void refl2(cplx a, cplx b, cplx* beta, cplx* tau, cplx* v2) {
-  double bx2 = cabs2(b);
-  double b0;
-  cplx t, sc;
-  householder(a, bx2, &b0, &t, &sc);
-  if (t.x == 0.0 && t.y == 0.0) {
-    *beta = a;
-    *tau = t;
-    *v2 = mk(0.0, 0.0);
-    return;
-  }
-  *beta = mk(b0, 0.0);
-  *tau = t;
-  *v2 = cmul(b, sc);
-}
-
-__global__ void __launch_bounds__(QR_THREADS)
-    hqr_kernel(cplx* const* __restrict__ Hs, cplx* const* __restrict__ Zs, cplx* const* __restrict__ Ws,
-               int n, int* __restrict__ status) {
-  __shared__ cplx D[QD * QD];
-  __shared__ cplx s_tau[QB], s_v2[QB];
-  __shared__ int s_red[QR_THREADS / 32];
-  __shared__ int s_l;
-  __shared__ cplx s_shift;
-
-  cplx* H = Hs[blockIdx.x];
-  cplx* Z = Zs[blockIdx.x];
-  cplx* W = Ws[blockIdx.x];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const double smlnum = SMLNUM_BASE * ((double)n / ULP);
-  const int itmax = 30 * max(10, n);       // per eigenvalue
-  const long long totmax = 30LL * n + 300;  // whole matrix (typical total is ~3n)
-  long long tot = 0;
-  auto h = [&](int r, int c) -> cplx& { return H[(size_t)c * n + r]; };
-
-  int i = n - 1;
-  int failed = 0;
-  while (i >= 0) {
-    int l = 0;
-    int its;
-    for (its = 0; its <= itmax && tot <= totmax; ++its, ++tot) {
-      // Deflation search: largest k in (l, i] with a negligible H[k][k-1].
-      int best = l;
-      for (int k = l + 1 + tid; k <= i; k += QR_THREADS) {
-        cplx sub = h(k, k - 1);
-        bool small = false;
-        double cs = cabs1(sub);
-        if (cs <= smlnum) {
-          small = true;
-        } else {
-          cplx dkm = h(k - 1, k - 1), dk = h(k, k);
-          double tst = cabs1(dkm) + cabs1(dk);
-          if (tst == 0.0) {
-            if (k - 2 >= 0) tst += fabs(h(k - 1, k - 2).x);
-            if (k + 1 <= n - 1) tst += fabs(h(k + 1, k).x);
-          }
-          if (cs <= ULP * tst) {
-            double a1 = cs, a2 = cabs1(h(k - 1, k));
-            double ab = fmax(a1, a2), ba = fmin(a1, a2);
-            double b1 = cabs1(dk), b2 = cabs1(csub(dkm, dk));
-            double aa = fmax(b1, b2), bb = fmin(b1, b2);
-            double s = aa + ab;
-            if (ba * (ab / s) <= fmax(smlnum, ULP * (bb * (aa / s)))) small = true;
-          }
-        }
-        if (small && k > best) best = k;
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
-      if (lane == 0) s_red[warp] = best;
-      __syncthreads();
-      if (tid == 0) {
-        int b = l;
-        for (int w = 0; w < QR_THREADS / 32; ++w) b = max(b, s_red[w]);
-        s_l = b;
-        if (b > l) h(b, b - 1) = mk(0.0, 0.0);
-      }
-      __syncthreads();
-      l = s_l;
-      if (l >= i) break;  // H[i][i] isolated
-      // Shift.
-      if (tid == 0) {
-        cplx t;
-        if (its == 10) {
-          double s = 0.75 * fabs(h(l + 1, l).x);
-          t = cadd(mk(s, 0.0), h(l, l));
-        } else if (its == 20) {
-          double s = 0.75 * fabs(h(i, i - 1).x);
-          t = cadd(mk(s, 0.0), h(i, i));
-        } else {
-          t = h(i, i);
-          cplx uu = cmul(csqrt(h(i - 1, i)), csqrt(h(i, i - 1)));
-          double s = cabs1(uu);
-          if (s != 0.0) {
-            cplx x = cscale(csub(h(i - 1, i - 1), t), 0.5);
-            double sx = cabs1(x);
-            s = fmax(s, sx);
-            cplx xs = cscale(x, 1.0 / s), us = cscale(uu, 1.0 / s);
-            cplx yv = cscale(csqrt(cadd(cmul(xs, xs), cmul(us, us))), s);
-            if (sx > 0.0) {
-              cplx xn = cscale(x, 1.0 / sx);
-              if (xn.x * yv.x + xn.y * yv.y < 0.0) yv = cneg(yv);
-            }
-            t = csub(t, cmul(uu, cdiv(uu, cadd(x, yv))));
-          }
-        }
-        s_shift = t;
-      }
-      __syncthreads();
-      const cplx shift = s_shift;
-      const int m = l;
-      // Single-shift sweep over steps k = m .. i-1, in chunks.
-      for (int k0 = m; k0 < i; k0 += QB) {
-        const int k1 = min(k0 + QB, i);  // steps k0..k1-1
-        const int ds = (k0 > m) ? k0 - 1 : m;
-        const int de = min(k1 + 1, i);
-        const int dn = de - ds + 1;
-        for (int idx = tid; idx < dn * dn; idx += QR_THREADS) {
-          int c = idx / dn, r = idx - c * dn;
-          D[c * QD + r] = h(ds + r, ds + c);
-        }
-        __syncthreads();
-        if (warp == 0) {
-          for (int k = k0; k < k1; ++k) {
-            if (lane == 0) {
-              cplx a, b;
-              if (k == m) {
-                a = csub(D[(k - ds) * QD + (k - ds)], shift);
-                b = D[(k - ds) * QD + (k + 1 - ds)];
-              } else {
-                a = D[(k - 1 - ds) * QD + (k - ds)];
-                b = D[(k - 1 - ds) * QD + (k + 1 - ds)];
-              }
-              cplx beta, tau, v2;
-              refl2(a, b, &beta, &tau, &v2);
-              if (k > m) {
-                D[(k - 1 - ds) * QD + (k - ds)] = beta;
-                D[(k - 1 - ds) * QD + (k + 1 - ds)] = mk(0.0, 0.0);
-              }
-              s_tau[k - k0] = tau;
-              s_v2[k - k0] = v2;
-            }
-            __syncwarp();
-            const cplx tau = s_tau[k - k0], v2 = s_v2[k - k0];
-            const cplx tauc = cconj(tau), v2c = cconj(v2);
-            // Row transform (rows k, k+1), columns k..de.
-            for (int j = k + lane; j <= de; j += 32) {
-              cplx x = D[(j - ds) * QD + (k - ds)], y = D[(j - ds) * QD + (k + 1 - ds)];
-              cplx sum = cmul(tauc, cadd(x, cmul(v2c, y)));
-              D[(j - ds) * QD + (k - ds)] = csub(x, sum);
-              D[(j - ds) * QD + (k + 1 - ds)] = csub(y, cmul(sum, v2));
-            }
-            __syncwarp();
-            // Column transform (cols k, k+1), rows ds..min(k+2, i).
-            const int re = min(k + 2, i);
-            for (int r = ds + lane; r <= re; r += 32) {
-              cplx p = D[(k - ds) * QD + (r - ds)], q = D[(k + 1 - ds) * QD + (r - ds)];
-              cplx sum = cmul(tau, cadd(p, cmul(v2, q)));
-              D[(k - ds) * QD + (r - ds)] = csub(p, sum);
-              D[(k + 1 - ds) * QD + (r - ds)] = csub(q, cmul(sum, v2c));
-            }
-            __syncwarp();
-          }
-        }
-        __syncthreads();
-        for (int idx = tid; idx < dn * dn; idx += QR_THREADS) {
-          int c = idx / dn, r = idx - c * dn;
-          h(ds + r, ds + c) = D[c * QD + r];
-        }
-        // Deferred updates outside the window.
-        const int nsteps = k1 - k0;
-        const int nright = n - 1 - de;      // columns de+1 .. n-1, rows k0..k1
-        const int nabove = ds;              // rows 0 .. ds-1, cols k0..k1
-        const int ntask = nright + nabove + n;
-        for (int task = tid; task < ntask; task += QR_THREADS) {
-          cplx e[QB + 1];
-          if (task < nright) {
-            const int j = de + 1 + task;
-            cplx* col = H + (size_t)j * n + k0;
-#pragma unroll
-            for (int s = 0; s <= QB; ++s)
-              if (s <= nsteps) e[s] = col[s];
-#pragma unroll
-            for (int s = 0; s < QB; ++s) {
-              if (s < nsteps) {
-                const cplx tauc = cconj(s_tau[s]), v2 = s_v2[s];
-                cplx sum = cmul(tauc, cadd(e[s], cmul(cconj(v2), e[s + 1])));
-                e[s] = csub(e[s], sum);
-                e[s + 1] = csub(e[s + 1], cmul(sum, v2));
-              }
-            }
-#pragma unroll
-            for (int s = 0; s <= QB; ++s)
-              if (s <= nsteps) col[s] = e[s];
-          } else {
-            int r;
-            cplx* base;
-            if (task < nright + nabove) {
-              r = task - nright;
-              base = H;
-            } else {
-              r = task - nright - nabove;
-              base = Z;
-            }
-#pragma unroll
-            for (int s = 0; s <= QB; ++s)
-              if (s <= nsteps) e[s] = base[(size_t)(k0 + s) * n + r];
-#pragma unroll
-            for (int s = 0; s < QB; ++s) {
-              if (s < nsteps) {
-                const cplx tau = s_tau[s], v2 = s_v2[s];
-                cplx sum = cmul(tau, cadd(e[s], cmul(v2, e[s + 1])));
-                e[s] = csub(e[s], sum);
-                e[s + 1] = csub(e[s + 1], cmul(sum, cconj(v2)));
-              }
-            }
-#pragma unroll
-            for (int s = 0; s <= QB; ++s)
-              if (s <= nsteps) base[(size_t)(k0 + s) * n + r] = e[s];
-          }
-        }
-        __syncthreads();
-      }
-    }
-    if (its > itmax || tot > totmax) {
-      failed = 1;
-      break;
-    }
-    i = l - 1;
-  }
-  __syncthreads();
-  for (int k = tid; k < n; k += QR_THREADS) W[k] = h(k, k);
-  if (tid == 0 && failed && status) status[blockIdx.x] = ST_ENOCONV;
-}
+constexpr double ULP = EIG_ULP;
+constexpr double SMLNUM_BASE = EIG_SAFMIN;
 
 // ---------------------------------------------------------------------------
 // 3. Eigenvectors of the triangular Schur factor
@@ -550,16 +284,6 @@ void hessenberg_batched(cplx* const* d_H, cplx* const* d_Z, int batch, int n, cu
   else if (n <= 512) launch_hess<16>(d_H, d_Z, batch, n, st);
   else if (n <= 1024) launch_hess<32>(d_H, d_Z, batch, n, st);
   else throw StatusError(ST_EINVAL, "eigensolver supports n <= 1024");
-  VRC_CUDA_CHECK(cudaGetLastError());
-}
-
-void schur_batched(cplx* const* d_H, cplx* const* d_Z, cplx* const* d_W, int batch, int n, int* d_status,
-                   cudaStream_t st) {
-  if (batch <= 0) return;
-  for (int b0 = 0; b0 < batch; b0 += 65535) {
-    int nb = min(65535, batch - b0);
-    hqr_kernel<<<nb, QR_THREADS, 0, st>>>(d_H + b0, d_Z + b0, d_W + b0, n, d_status ? d_status + b0 : nullptr);
-  }
   VRC_CUDA_CHECK(cudaGetLastError());
 }
 

@@ -5,8 +5,10 @@
 #include "engine.h"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <complex>
+#include <cstdlib>
 #include <cstring>
 #include <tuple>
 #include <list>
@@ -56,8 +58,20 @@ BlockPool::~BlockPool() {
   for (void* c : chunks_) cudaFree(c);
 }
 
+namespace {
+double g_host_alloc_ms = 0.0;  // host time spent in cudaMalloc/cudaFree
+struct AllocTimer {
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+  ~AllocTimer() {
+    g_host_alloc_ms +=
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+};
+}  // namespace
+
 void* BlockPool::get() {
   if (free_.empty()) {
+    AllocTimer at;
     size_t per = std::max<size_t>(1, (size_t)(64u << 20) / bytes_);
     if (per > 256) per = 256;
     void* chunk = nullptr;
@@ -141,11 +155,13 @@ void Engine::set_profiling(bool on) {
 }
 std::map<std::string, Engine::FamStat>& Engine::fam_stats() {
   sync();
+  fam_["host_alloc"].ms = g_host_alloc_ms - alloc_ms0_;
   return fam_;
 }
 void Engine::reset_fam_stats() {
   sync();
   fam_.clear();
+  alloc_ms0_ = g_host_alloc_ms;
 }
 
 Engine::Prof::Prof(Engine& eng, const char* f, double fl, double by, int nlaunch)
@@ -197,6 +213,7 @@ void* Engine::stage(const void* data, size_t nbytes) {
 void* Engine::workspace(size_t nbytes) {
   if (nbytes > ws_cap_) {
     sync();
+    AllocTimer at;
     if (ws_) cudaFree(ws_);
     ws_ = nullptr;
     size_t cap = nbytes + nbytes / 4;
@@ -715,7 +732,8 @@ void Engine::assemble(std::vector<SampleReq>& reqs, std::vector<int>* status) {
 // ---------------------------------------------------------------------------
 void Engine::eig(std::vector<EigReq>& reqs, int n, std::vector<int>* status) {
   if (reqs.empty()) return;
-  const size_t per = (size_t)3 * n * n + 2 * (size_t)((n + 15) / 16 * 16);
+  const size_t logc = schur_log_bytes(n) / 16;  // rotation log, complex units
+  const size_t per = (size_t)3 * n * n + 2 * (size_t)((n + 15) / 16 * 16) + logc;
   size_t chunk = std::max<size_t>(1, batch_budget_bytes() / (per * 16));
   chunk = std::min<size_t>(chunk, 16384);
   if (status && status->size() < reqs.size()) status->resize(reqs.size(), 0);
@@ -723,6 +741,7 @@ void Engine::eig(std::vector<EigReq>& reqs, int n, std::vector<int>* status) {
     const size_t B = std::min(chunk, reqs.size() - c0);
     cplx* ws = (cplx*)workspace(B * per * 16);
     std::vector<cplx*> H(B), Z(B), Y(B), lam(B), ig(B), W(B), V(B), gam(B);
+    std::vector<void*> logs(B);
     std::vector<GemmDesc> g;
     for (size_t b = 0; b < B; ++b) {
       cplx* base = ws + b * per;
@@ -731,6 +750,7 @@ void Engine::eig(std::vector<EigReq>& reqs, int n, std::vector<int>* status) {
       Y[b] = base + 2 * (size_t)n * n;
       lam[b] = base + 3 * (size_t)n * n;
       ig[b] = lam[b] + (n + 15) / 16 * 16;
+      logs[b] = ig[b] + (n + 15) / 16 * 16;
       const EigReq& r = reqs[c0 + b];
       W[b] = r.W;
       V[b] = r.V;
@@ -748,8 +768,33 @@ void Engine::eig(std::vector<EigReq>& reqs, int n, std::vector<int>* status) {
     int* dstat = (int*)bytes(B * sizeof(int));
     VRC_CUDA_CHECK(cudaMemsetAsync(dstat, 0, B * sizeof(int), stream_));
     {
-      Prof pr(*this, "schur_qr", 80.0 * nn3 * B, 4.0 * mbytes * B);
-      schur_batched(upload(H), upload(Z), upload(lam), (int)B, n, dstat, stream_);
+      cplx* const* dH = upload(H);
+      cplx* const* dZ = upload(Z);
+      cplx* const* dL = upload(lam);
+      void* const* dG = upload(logs);
+      {
+        Prof pr(*this, "schur_qr", 80.0 * nn3 * B, 4.0 * mbytes * B);
+        schur_batched(dH, dZ, dL, dG, (int)B, n, dstat, stream_, SCHUR_ITERATE);
+      }
+      Prof pr(*this, "schur_replay", 0.0, 4.0 * mbytes * B, 2);
+      schur_batched(dH, dZ, dL, dG, (int)B, n, dstat, stream_, SCHUR_REPLAY);
+    }
+    if (std::getenv("VRC_QR_STATS")) {
+      // diagnostic: per-matrix QR counters from the rotation-log headers
+      double tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      for (size_t b = 0; b < B; ++b) {
+        int hh[4];
+        long long tt[4];
+        VRC_CUDA_CHECK(cudaMemcpyAsync(hh, logs[b], sizeof(hh), cudaMemcpyDeviceToHost, stream_));
+        VRC_CUDA_CHECK(cudaMemcpyAsync(tt, (char*)logs[b] + 16, sizeof(tt), cudaMemcpyDeviceToHost, stream_));
+        sync();
+        for (int q = 0; q < 4; ++q) tot[q] += hh[q], tot[4 + q] += (double)tt[q];
+      }
+      fprintf(stderr,
+              "[vrc qr] n=%d matrices=%zu per matrix: sweeps=%.1f rounds=%.0f rotation slots=%.0f (%.2f n^2) "
+              "Mcycles defl=%.2f shift=%.2f rounds=%.2f far=%.2f\n",
+              n, B, tot[0] / B, tot[2] / B, tot[1] / B, tot[1] / B / ((double)n * n), tot[4] / B / 1e6,
+              tot[5] / B / 1e6, tot[6] / B / 1e6, tot[7] / B / 1e6);
     }
     {
       Prof pr(*this, "trevc", (4.0 / 3.0) * nn3 * B, 1.5 * mbytes * B);

@@ -271,6 +271,7 @@ class Engine {
   void* ws_ = nullptr;
   size_t ws_cap_ = 0;
   bool profiling_ = false;
+  double alloc_ms0_ = 0.0;
   struct PendingProf {
     const char* fam;
     cudaEvent_t a, b;

@@ -24,8 +24,15 @@ void zinv_batched(cplx* const* d_mats, int batch, int n, int* d_status, cudaStre
 
 // ---- eigensolver ---------------------------------------------------------------
 void hessenberg_batched(cplx* const* d_H, cplx* const* d_Z, int batch, int n, cudaStream_t st);
-void schur_batched(cplx* const* d_H, cplx* const* d_Z, cplx* const* d_W, int batch, int n, int* d_status,
-                   cudaStream_t st);
+// Complex Schur form + Schur vectors.  d_logs: one rotation-log buffer of
+// schur_log_bytes(n) bytes per matrix (device scratch, contents overwritten).
+// parts: SCHUR_ITERATE (QR sweeps on the active windows, rotations logged),
+// SCHUR_REPLAY (logged rotations applied to Z and to H outside the windows),
+// or both, in that order.
+size_t schur_log_bytes(int n);
+constexpr int SCHUR_ITERATE = 1, SCHUR_REPLAY = 2;
+void schur_batched(cplx* const* d_H, cplx* const* d_Z, cplx* const* d_W, void* const* d_logs, int batch, int n,
+                   int* d_status, cudaStream_t st, int parts = SCHUR_ITERATE | SCHUR_REPLAY);
 void trevc_batched(cplx* const* d_T, cplx* const* d_Y, int batch, int n, cudaStream_t st);
 void vecnorm_batched(cplx* const* d_X, int batch, int n, cudaStream_t st);
 

@@ -7,8 +7,9 @@
 // vrc_eig_noalloc runs the same eigensolver kernels as vrc_eig on one
 // n x n matrix (n <= VRC_EIG_NOALLOC_MAX_N) with the caller's device buffers
 // and a fixed scratch area that is part of the library image: a file-scope
-// __device__ array of 3 * 256 * 256 complex128 values plus a few words
-// (about 3 MiB on every GPU that loads the library, held until exit).
+// __device__ array holding three 256 x 256 complex128 work matrices and the
+// QR rotation log (about 22 MiB on every GPU that loads the library, held
+// until exit).
 //
 // The scratch is shared by every call in the process on that device and
 // keeps the last call's contents; the entry point overwrites or clears all
@@ -36,7 +37,14 @@ constexpr size_t kOffY = kOffZ + kMat;
 constexpr size_t kOffPtr = kOffY + kMat;          // 8 pointers
 constexpr size_t kOffDesc = kOffPtr + 8 * sizeof(void*);
 constexpr size_t kOffStatus = kOffDesc + 256;     // one int
-constexpr size_t kScratchBytes = kOffStatus + 256;
+constexpr size_t kOffLog = kOffStatus + 256;      // QR rotation log
+// log capacity for n = kMaxN: 64-byte header, sweep records of 32 bytes
+// (bounded here by half the rotation capacity + 256, more than the iteration
+// cap allows) and 6n^2+64 rotations of 32 bytes (checked against
+// schur_log_bytes at run time)
+constexpr size_t kRotCap = (size_t)6 * kMaxN * kMaxN + 64;
+constexpr size_t kLogBytes = (64 + (kRotCap / 2 + 256) * 32 + kRotCap * 32 + 255) / 256 * 256;
+constexpr size_t kScratchBytes = kOffLog + kLogBytes;
 
 static __device__ __align__(256) unsigned char g_eig_scratch[kScratchBytes];
 
@@ -50,6 +58,7 @@ __global__ void noalloc_setup_kernel(cplx* W, cplx* lam) {
   p[2] = reinterpret_cast<cplx*>(base + kOffY);
   p[3] = lam;
   p[4] = W;
+  p[5] = reinterpret_cast<cplx*>(base + kOffLog);
   vrc::GemmDesc* d = reinterpret_cast<vrc::GemmDesc*>(base + kOffDesc);
   d->A = p[1];
   d->B = p[2];
@@ -92,6 +101,10 @@ extern "C" int vrc_eig_noalloc(int n, const vrc_complex* A, vrc_complex* W, vrc_
   }
   unsigned char* base = scratch_address(dev);
   if (!base) return VRC_ECUDA;
+  if (vrc::schur_log_bytes(kMaxN) > kLogBytes) {
+    fprintf(stderr, "vrc_eig_noalloc: rotation-log scratch too small\n");
+    return VRC_EINVAL;
+  }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   try {
     cplx* H = reinterpret_cast<cplx*>(base + kOffH);
@@ -107,7 +120,8 @@ extern "C" int vrc_eig_noalloc(int n, const vrc_complex* A, vrc_complex* W, vrc_
     noalloc_setup_kernel<<<1, 1, 0, st>>>(reinterpret_cast<cplx*>(W), reinterpret_cast<cplx*>(lam));
     VRC_CUDA_CHECK(cudaGetLastError());
     vrc::hessenberg_batched(pH, pZ, 1, n, st);
-    vrc::schur_batched(pH, pZ, pLam, 1, n, status, st);
+    void* const* pLog = reinterpret_cast<void* const*>(pH + 5);
+    vrc::schur_batched(pH, pZ, pLam, pLog, 1, n, status, st);
     vrc::trevc_batched(pH, pY, 1, n, st);
     vrc::zgemm_batched(desc, 1, n, vrc::mk(1, 0), vrc::mk(0, 0), 0.0, st);  // W = Z Y
     vrc::vecnorm_batched(pW, 1, n, st);
