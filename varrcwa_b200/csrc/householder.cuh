@@ -15,11 +15,15 @@ __device__ __forceinline__ void householder(cplx alpha, double xnorm2, double* b
     *scale = mk(0.0, 0.0);
     return;
   }
-  double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xnorm2);
-  double b = alpha.x >= 0.0 ? -nrm : nrm;
+  const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xnorm2);
+  const double b = alpha.x >= 0.0 ? -nrm : nrm;
+  // alpha - beta = (alpha.x + sign(alpha.x) nrm, alpha.y): |real part| >= nrm > 0,
+  // so both reciprocals are safe; they are independent and overlap.
+  const double ux = alpha.x - b;
+  const double rb = 1.0 / b, rd = 1.0 / (ux * ux + alpha.y * alpha.y);
   *beta = b;
-  *tau = mk((b - alpha.x) / b, -alpha.y / b);
-  *scale = cinv(mk(alpha.x - b, alpha.y));
+  *tau = mk(-ux * rb, -alpha.y * rb);
+  *scale = mk(ux * rd, -alpha.y * rd);
 }
 
 // Two-element reflector for (a, b): returns the new leading entry, tau and

@@ -10,11 +10,12 @@
 // all row transforms, synchronises, then all column transforms together with
 // each bulge's next reflector.  Rounds run in chunks of QB inside a diagonal
 // window D held in shared memory; after a chunk the rest of the active
-// window is updated by one thread per row or column, which applies the
-// chunk's rounds in order with its entries in a sliding register window
-// (SweepRing).  Rows above the window, columns right of it and all of Z
-// are not touched here: every sweep's rotations are logged round-major and
-// replayed afterwards (qr_replay_rows_kernel / qr_replay_cols_kernel).  For
+// window is updated by one thread per row or column, which carries a value
+// down each bulge's chain of the chunk (carry_chain).  Rows above the
+// window, columns right of it and all of Z are not touched here: every
+// sweep's rotations are logged round-major and replayed afterwards, whole
+// rounds at a time from a sliding register ring (qr_replay_rows_kernel /
+// qr_replay_cols_kernel).  For
 // any entry, eager in-window updates precede deferred column transforms,
 // which precede deferred row transforms (the window's bottom only moves up
 // and windows never straddle a zero subdiagonal), so the replay reproduces
@@ -35,7 +36,6 @@ constexpr int NBMAX = QR_THREADS / 32;           // bulges per sweep (one warp e
 constexpr int QB = 32;                           // rounds per chunk
 constexpr int QD = QB + 3 * (NBMAX - 1) + 3;     // diagonal window size (56)
 constexpr size_t QR_SMEM = (size_t)(QD * QD + 2 * NBMAX * QB) * sizeof(cplx);
-constexpr int FAR_NBG = 2;  // bulges per pass of the in-window update (register budget)
 
 struct QrLogHeader {
   int nsweeps, nrot;
@@ -171,82 +171,33 @@ __device__ __forceinline__ void rotate2(cplx& a, cplx& b, cplx tau, cplx v2) {
   }
 }
 
-// Applies consecutive rounds of a group of ng <= NBG bulges (3 positions
-// apart) to one vector x: a column under row transforms (ROWOP, entry c at
-// x[c * stride] is row c) or a row under column transforms (entry c is
-// column c).  In round t (0 <= t < cnt), bulge g of the group acts on the
-// pair (k, k+1), k = kb + t - 3g, when lo <= k <= hi - 1.  The entries in
-// use slide down with t, so they live in a ring of P registers indexed by
-// compile-time slots (round loops are unrolled by P): each round prefetches
-// the entry PF rounds ahead and retires the one the group's trailing bulge
-// has passed; the group's rotations within a round touch disjoint pairs and
-// run independently.  begin() loads the first entries, run() applies rounds
-// [t0, t1) (t0 a multiple of P) and stores everything back with the last
-// round, so a caller can stage rotations between run() calls.
-template <int NBG, int PF, bool ROWOP>
-struct SweepRing {
-  static constexpr int L = 3 * (NBG - 1);  // retire lag
-  static constexpr int P = L + PF + 3;     // ring size (> L + PF + 1)
-  cplx w[P];
-  cplx* x;
-  size_t stride;
-  int kb, lo, hi, rmin, cnt;
-
-  __device__ __forceinline__ void begin(cplx* x_, size_t stride_, int kb_, int lo_, int hi_, int ng, int cnt_) {
-    x = x_;
-    stride = stride_;
-    kb = kb_;
-    lo = lo_;
-    hi = hi_;
-    rmin = -3 * (ng - 1);
-    cnt = cnt_;
-    if (cnt <= 0) return;
+// Carries one value down a chain of cnt rotations on consecutive index
+// pairs (k0, k0+1), (k0+1, k0+2), ...: row transforms on a column (rowop,
+// entries p0[t], stride 1) or column transforms on a row (stride n).  The
+// entries are fetched eight at a time ahead of use.
+__device__ __forceinline__ void carry_chain(cplx* p0, size_t stride, int cnt, const cplx* taus, const cplx* v2s,
+                                            bool rowop) {
+  cplx c = p0[0];
+  for (int t0 = 0; t0 < cnt; t0 += 8) {
+    cplx q[8];
 #pragma unroll
-    for (int q = -L; q <= PF; ++q) {  // entries of round 0 plus the prefetch
-      const int c = kb + q;
-      if (q >= rmin && c >= lo && c <= hi) w[(q + P) % P] = x[(size_t)c * stride];
-    }
-  }
-
-  // rot(t, g, &tau, &v2) must be safe to call for every g < NBG and t in
-  // [t0, t1); its value is used only for active pairs of the first ng bulges.
-  template <class Rot>
-  __device__ __forceinline__ void run(int t0, int t1, Rot rot) {
-    t1 = min(t1, cnt);
-    for (int tb = t0; tb < t1; tb += P) {
+    for (int u = 0; u < 8; ++u)
+      if (t0 + u < cnt) q[u] = p0[(size_t)(t0 + u + 1) * stride];
 #pragma unroll
-      for (int tt = 0; tt < P; ++tt) {
-        const int t = tb + tt;
-        if (t < t1) {
-          const int cb = kb + t;
-          {
-            const int c = cb + 1 + PF;
-            if (c >= lo && c <= hi) w[(tt + 1 + PF) % P] = x[(size_t)c * stride];
-          }
-#pragma unroll
-          for (int g = 0; g < NBG; ++g) {
-            cplx tau, v2;
-            rot(t, g, &tau, &v2);
-            const int k = cb - 3 * g;
-            if (3 * g <= -rmin && k >= lo && k <= hi - 1)
-              rotate2<ROWOP>(w[(tt - 3 * g + 2 * P) % P], w[(tt - 3 * g + 1 + 2 * P) % P], tau, v2);
-          }
-          {
-            const int q = t - L, c = cb - L;
-            if (q >= rmin && c >= lo && c <= hi) x[(size_t)c * stride] = w[(tt - L + 2 * P) % P];
-          }
-          if (t == cnt - 1) {
-#pragma unroll
-            for (int d = 1; d <= L + 1; ++d) {  // entries t-L+1 .. t+1 still held
-              const int q = t - L + d, c = cb - L + d;
-              if (q >= rmin && c >= lo && c <= hi) x[(size_t)c * stride] = w[(tt - L + d + 2 * P) % P];
-            }
-          }
-        }
+    for (int u = 0; u < 8; ++u) {
+      if (t0 + u < cnt) {
+        cplx b = q[u];
+        if (rowop)
+          rotate2<true>(c, b, taus[t0 + u], v2s[t0 + u]);
+        else
+          rotate2<false>(c, b, taus[t0 + u], v2s[t0 + u]);
+        p0[(size_t)(t0 + u) * stride] = c;
+        c = b;
       }
     }
   }
-};
+  p0[(size_t)cnt * stride] = c;
+}
 
 __global__ void __launch_bounds__(QR_THREADS, 2)
     hqr_kernel(cplx* const* __restrict__ Hs, void* const* __restrict__ logs, cplx* const* __restrict__ Ws, int n,
@@ -446,28 +397,18 @@ __global__ void __launch_bounds__(QR_THREADS, 2)
           rot[2 * ri + 1] = s_v2[b * QB + u];
         }
         // Rest of the active window: columns de+1..i (row transforms) and rows
-        // m..ds-1 (column transforms), FAR_NBG bulges at a time, leading first.
+        // m..ds-1 (column transforms), one bulge chain at a time, leading
+        // bulge first (the order of every pair of conflicting rotations).
         const int nright = i - de, nabove = ds - m;
         for (int task = tid; task < nright + nabove; task += QR_THREADS) {
           const bool rowop = task < nright;
-          for (int b0 = 0; b0 < nb; b0 += FAR_NBG) {
-            const int ng = min(FAR_NBG, nb - b0);
-            const int kb = m + r0 - 3 * b0;
-            const cplx* taus = s_tau + b0 * QB;
-            const cplx* v2s = s_v2 + b0 * QB;
-            auto rf = [&](int t, int g, cplx* tau, cplx* v2) {
-              *tau = taus[g * QB + t];
-              *v2 = v2s[g * QB + t];
-            };
-            if (rowop) {
-              SweepRing<FAR_NBG, 1, true> ring;
-              ring.begin(H + (size_t)(de + 1 + task) * n, 1, kb, m, i, ng, nr);
-              ring.run(0, nr, rf);
-            } else {
-              SweepRing<FAR_NBG, 1, false> ring;
-              ring.begin(H + (m + task - nright), (size_t)n, kb, m, i, ng, nr);
-              ring.run(0, nr, rf);
-            }
+          for (int b = 0; b < nb; ++b) {
+            const int ra0 = max(r0, 3 * b), ra1 = min(r1, 3 * b + (i - m));
+            if (ra1 <= ra0) continue;
+            const int k0 = m + ra0 - 3 * b;
+            cplx* p0 = rowop ? H + (size_t)(de + 1 + task) * n + k0 : H + (size_t)k0 * n + (m + task - nright);
+            carry_chain(p0, rowop ? 1 : (size_t)n, ra1 - ra0, s_tau + b * QB + (ra0 - r0), s_v2 + b * QB + (ra0 - r0),
+                        rowop);
           }
         }
         __syncthreads();
@@ -506,7 +447,11 @@ __global__ void __launch_bounds__(QR_THREADS, 2)
 // memory in slabs of RS rounds and read as broadcasts.  A thread's entries
 // arrive PFD rounds ahead through 16-byte cp.async copies into its own
 // shared-memory slots (the rounds are short, so register prefetch cannot
-// cover the memory latency), then move into a register ring as in SweepRing.
+// cover the memory latency), then move into a ring of registers indexed by
+// compile-time slots (round loops are unrolled by the ring size): each round
+// takes in the entry the leading bulge reaches and retires the one the
+// trailing bulge has passed; the group's rotations within a round touch
+// disjoint pairs and run independently.
 constexpr int RP_THREADS = 128;
 constexpr int RP_NBG = 4;  // bulges per register ring
 constexpr int RP_PFD = 8;  // prefetch depth in rounds
