@@ -19,7 +19,7 @@ CSRC = PKG / "csrc"
 BUILD = ROOT / "_build"
 LIB = PKG / "libvrc.so"
 
-SOURCES = ["gemm.cu", "inverse.cu", "eig.cu", "qr.cu", "assembly.cu", "segment.cu", "engine.cu", "drivers.cu",
+SOURCES = ["gemm.cu", "inverse.cu", "eig.cu", "hessenberg.cu", "qr.cu", "assembly.cu", "segment.cu", "engine.cu", "drivers.cu",
            "capi.cu", "noalloc.cu"]
 HEADERS = ["common.cuh", "kernels.h", "engine.h", "householder.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -259,18 +259,14 @@ static int eig_common(vrc_context* ctx, int batch, int n, const vrc_complex* P, 
     vrc::Engine& E = *ctx->eng;
     const size_t nn = (size_t)n * n;
     std::vector<cplx*> Pd(batch), Qd(batch), Wd(batch), Vd(batch), gd(batch), ld(batch);
-    std::vector<cplx> eye;
-    if (!Q) {
-      eye.assign(nn, vrc::mk(0, 0));
-      for (int i = 0; i < n; ++i) eye[(size_t)i * n + i] = vrc::mk(1, 0);
-    }
     std::vector<vrc::Engine::EigReq> req;
     for (int b = 0; b < batch; ++b) {
       Pd[b] = E.mat(n); Qd[b] = E.mat(n); Wd[b] = E.mat(n); Vd[b] = E.mat(n); gd[b] = E.vec(n); ld[b] = E.vec(n);
       VRC_CUDA_CHECK(cudaMemcpyAsync(Pd[b], P + (size_t)b * nn, nn * 16, cudaMemcpyHostToDevice, E.stream()));
-      VRC_CUDA_CHECK(cudaMemcpyAsync(Qd[b], Q ? (const void*)(Q + (size_t)b * nn) : (const void*)eye.data(), nn * 16,
-                                     cudaMemcpyHostToDevice, E.stream()));
-      vrc::Engine::EigReq r{Pd[b], Qd[b], Wd[b], Vd[b], nullptr, nullptr, gd[b]};
+      if (Q)
+        VRC_CUDA_CHECK(cudaMemcpyAsync(Qd[b], Q + (size_t)b * nn, nn * 16, cudaMemcpyHostToDevice, E.stream()));
+      // without Q the eigenpairs of P itself (no product, so no rounding)
+      vrc::Engine::EigReq r{Pd[b], Q ? Qd[b] : nullptr, Wd[b], Vd[b], nullptr, nullptr, gd[b]};
       r.lam = ld[b];
       req.push_back(r);
     }

@@ -13,6 +13,8 @@
 //   4. vecnorm_kernel  X = Z Y is formed by the GEMM; each column is scaled to
 //                    unit 2-norm with its largest component real (the zgeev
 //                    convention).
+#include <cstdlib>
+
 #include "common.cuh"
 #include "householder.cuh"
 #include "kernels.h"
@@ -280,6 +282,10 @@ void launch_hess(cplx* const* H, cplx* const* Z, int batch, int n, cudaStream_t 
 
 void hessenberg_batched(cplx* const* d_H, cplx* const* d_Z, int batch, int n, cudaStream_t st) {
   if (batch <= 0) return;
+  if (hessenberg_cluster_fits(n) && !std::getenv("VRC_HESS_SINGLE_CTA")) {
+    hessenberg_cluster_batched(d_H, d_Z, batch, n, st);
+    return;
+  }
   if (n <= 256) launch_hess<8>(d_H, d_Z, batch, n, st);
   else if (n <= 512) launch_hess<16>(d_H, d_Z, batch, n, st);
   else if (n <= 1024) launch_hess<32>(d_H, d_Z, batch, n, st);

@@ -755,9 +755,19 @@ void Engine::eig(std::vector<EigReq>& reqs, int n, std::vector<int>* status) {
       W[b] = r.W;
       V[b] = r.V;
       gam[b] = r.gam;
-      g.push_back({r.P, r.Q, H[b], nullptr, nullptr, nullptr});
+      if (r.Q) g.push_back({r.P, r.Q, H[b], nullptr, nullptr, nullptr});
     }
     gemm(g, n, mk(1, 0), mk(0, 0), 0.0);  // PQ = P*Q
+    {
+      // a request without Q asks for the eigenpairs of P itself
+      std::vector<cplx*> src, dst;
+      for (size_t b = 0; b < B; ++b)
+        if (!reqs[c0 + b].Q) {
+          src.push_back(const_cast<cplx*>(reqs[c0 + b].P));
+          dst.push_back(H[b]);
+        }
+      if (!src.empty()) copy(src, dst, n);
+    }
     // nominal LAPACK counts (real flops): zgehrd 40/3 n^3 + zunghr 16/3 n^3,
     // complex Schur with Z ~ 80 n^3, ztrevc 4/3 n^3
     const double nn3 = (double)n * n * n, mbytes = 16.0 * n * (double)n;
@@ -810,7 +820,8 @@ void Engine::eig(std::vector<EigReq>& reqs, int n, std::vector<int>* status) {
       gamma_batched(upload(lamc), upload(gam), upload(ig), (int)B, n, stream_);
     }
     g.clear();
-    for (size_t b = 0; b < B; ++b) g.push_back({reqs[c0 + b].Q, W[b], V[b], nullptr, nullptr, ig[b]});
+    for (size_t b = 0; b < B; ++b)
+      if (reqs[c0 + b].Q) g.push_back({reqs[c0 + b].Q, W[b], V[b], nullptr, nullptr, ig[b]});
     gemm(g, n, mk(1, 0), mk(0, 0), 0.0);  // V = Q W diag(1/gamma)
     std::vector<cplx*> srcs, dsts;
     for (size_t b = 0; b < B; ++b) {

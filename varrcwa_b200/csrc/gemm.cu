@@ -5,11 +5,11 @@
 // for square column-major n x n operands (every contraction of the hot path
 // is square: projections, star products, perturbation terms, P*Q).  One CTA
 // computes a 64 x 64 complex tile; operands are staged through shared memory
-// by 16-byte cp.async copies in a 3-stage pipeline.  The complex product is
-// the 4-real-product form (Cr += Ar Br - Ai Bi, Ci += Ar Bi + Ai Br), which
-// keeps the rounding of a standard complex GEMM (cuBLAS Zgemm3m used by the
-// reference GPU path, src/gpu/types.cuh:33, changes rounding; Eigen/MKL on
-// the CPU path do not).
+// by 16-byte cp.async copies in a 3-stage pipeline.  The complex product
+// uses three real products (P1 = Ar Br, P2 = Ai Bi, P3 = (Ar+Ai)(Br+Bi);
+// Cr = P1 - P2, Ci = P3 - P1 - P2), as cuBLAS Zgemm3m on the reference GPU
+// path (src/gpu/types.cuh:33): a quarter fewer tensor-core products than the
+// four-product form, with the normwise-stable error bound of the 3M method.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -42,7 +42,7 @@ __device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, doubl
       : "d"(a0), "d"(a1), "d"(b0));
 }
 
-__global__ void __launch_bounds__(NTHREADS)
+__global__ void __launch_bounds__(NTHREADS, 2)
     zgemm_kernel(const GemmDesc* __restrict__ descs, int n, cplx alpha, cplx beta, double delta) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx* As = reinterpret_cast<cplx*>(smem_raw);        // [STAGES][BK][LDA]
@@ -81,13 +81,13 @@ __global__ void __launch_bounds__(NTHREADS)
     }
   };
 
-  double acc_r[2][2][4], acc_i[2][2][4];
+  double acc1[2][2][4], acc2[2][2][4], acc3[2][2][4];
 #pragma unroll
   for (int a = 0; a < 2; ++a)
 #pragma unroll
     for (int b = 0; b < 2; ++b)
 #pragma unroll
-      for (int c = 0; c < 4; ++c) acc_r[a][b][c] = acc_i[a][b][c] = 0.0;
+      for (int c = 0; c < 4; ++c) acc1[a][b][c] = acc2[a][b][c] = acc3[a][b][c] = 0.0;
 
 #pragma unroll
   for (int s = 0; s < STAGES - 1; ++s) {
@@ -119,10 +119,9 @@ __global__ void __launch_bounds__(NTHREADS)
       for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
         for (int nt = 0; nt < 2; ++nt) {
-          dmma(acc_r[mt][nt], af[mt][0].x, af[mt][1].x, bf[nt].x);
-          dmma(acc_r[mt][nt], -af[mt][0].y, -af[mt][1].y, bf[nt].y);
-          dmma(acc_i[mt][nt], af[mt][0].x, af[mt][1].x, bf[nt].y);
-          dmma(acc_i[mt][nt], af[mt][0].y, af[mt][1].y, bf[nt].x);
+          dmma(acc1[mt][nt], af[mt][0].x, af[mt][1].x, bf[nt].x);
+          dmma(acc2[mt][nt], af[mt][0].y, af[mt][1].y, bf[nt].y);
+          dmma(acc3[mt][nt], af[mt][0].x + af[mt][0].y, af[mt][1].x + af[mt][1].y, bf[nt].x + bf[nt].y);
         }
     }
   }
@@ -138,7 +137,8 @@ __global__ void __launch_bounds__(NTHREADS)
         int row = m0 + wm * 32 + mt * 16 + g + ((c >> 1) << 3);
         int col = n0 + wn * 16 + nt * 8 + tig * 2 + (c & 1);
         if (row < n && col < n) {
-          cplx v = mk(acc_r[mt][nt][c], acc_i[mt][nt][c]);
+          const double p1 = acc1[mt][nt][c], p2 = acc2[mt][nt][c];
+          cplx v = mk(p1 - p2, acc3[mt][nt][c] - p1 - p2);
           v = cmul(alpha, v);
           if (d.rs) v = cmul(d.rs[row], v);
           if (d.cs) v = cmul(v, d.cs[col]);

@@ -1,0 +1,272 @@
+// Hessenberg reduction H = Q^H A Q with Q accumulated, one thread-block
+// cluster of HC_CS CTAs per matrix and the matrix held on chip.
+//
+// The single-CTA reduction streams the trailing matrix through L2/HBM twice
+// per column (BLAS-2), which makes it memory bound.  Here CTA c of the
+// cluster keeps columns c, c + HC_CS, c + 2 HC_CS, ... in its shared memory,
+// so every pass runs out of shared memory; the only cross-CTA data are the
+// reflector v (written by the owner of column k into every CTA) and the
+// partial products y = A[:, J] v (each CTA writes its part into every CTA,
+// which sums them), exchanged through distributed shared memory between two
+// cluster barriers per column.  Buffers alternate by the parity of k, so a
+// CTA one step ahead never overwrites data a slower CTA still reads.
+//
+// Per column k (J = [k+1, n), v = (1, v_2, ...) on J, tau):
+//   y = A[:, J] v,  u_j = v^H A[J, j],  s = v^H y_J,  z_j = u_j - tau s conj(v_j)
+//   A[:, J] -= y (tau v^H);  A[J, j] -= v (conj(tau) z_j)
+// (the two-sided application of I - tau v v^H fused into one rank-2 update,
+// the published Householder reduction of Golub & Van Loan 7.4.3 in complex
+// form).  Afterwards every CTA forms its own columns of
+// Q = H_0 H_1 ... H_{n-3} by backward accumulation, reading the reflectors
+// stored below the subdiagonal of the written-back matrix.
+#include <cooperative_groups.h>
+
+#include "common.cuh"
+#include "householder.cuh"
+#include "kernels.h"
+
+namespace cg = cooperative_groups;
+
+namespace vrc {
+namespace {
+
+constexpr int HC_CS = 8;         // CTAs per cluster (portable maximum)
+constexpr int HC_THREADS = 256;  // one thread per matrix row: n <= HC_THREADS
+constexpr int HC_WARPS = HC_THREADS / 32;
+
+__device__ __forceinline__ cplx warp_sum_c(cplx v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+    v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+  }
+  return v;
+}
+
+struct HcLayout {
+  int w;                                  // columns per CTA
+  size_t a, vb, yp, tau, u, total;  // byte offsets
+};
+
+__host__ __device__ inline HcLayout hc_layout(int n) {
+  HcLayout L;
+  L.w = (n + HC_CS - 1) / HC_CS;
+  size_t o = 0;
+  L.a = o;
+  o += (size_t)L.w * n * sizeof(cplx);  // own columns, column-major, leading dimension n
+  L.vb = o;
+  o += 2 * (size_t)HC_THREADS * sizeof(cplx);  // reflector, two parities
+  L.yp = o;
+  o += 2 * (size_t)HC_CS * HC_THREADS * sizeof(cplx);  // partial y from every CTA, two parities
+  L.tau = o;
+  o += (size_t)HC_THREADS * sizeof(cplx);  // tau of every column
+  L.u = o;
+  o += 2 * (size_t)L.w * sizeof(cplx);  // u (then b) and a per own column
+  L.total = o;
+  return L;
+}
+
+// Block-wide sum of one complex value per thread (all threads get the sum).
+__device__ __forceinline__ cplx block_sum(cplx v, cplx* scratch) {
+  v = warp_sum_c(v);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();  // scratch free
+  if (lane == 0) scratch[warp] = v;
+  __syncthreads();
+  cplx s = mk(0.0, 0.0);
+#pragma unroll
+  for (int q = 0; q < HC_WARPS; ++q) s = cadd(s, scratch[q]);
+  return s;
+}
+
+__global__ void __cluster_dims__(HC_CS, 1, 1) __launch_bounds__(HC_THREADS, 1)
+    hess_cluster_kernel(cplx* const* __restrict__ Hs, cplx* const* __restrict__ Zs, int n) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ cplx s_red[HC_WARPS];
+  __shared__ cplx s_scale;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = (int)cluster.block_rank();
+  const HcLayout L = hc_layout(n);
+  cplx* A = reinterpret_cast<cplx*>(smem_raw + L.a);  // local column jl is global column rank + HC_CS*jl
+  cplx* vb = reinterpret_cast<cplx*>(smem_raw + L.vb);
+  cplx* yp = reinterpret_cast<cplx*>(smem_raw + L.yp);
+  cplx* taus = reinterpret_cast<cplx*>(smem_raw + L.tau);
+  cplx* us = reinterpret_cast<cplx*>(smem_raw + L.u);  // u_j, then b_j
+  cplx* ca = us + L.w;                                 // a_j
+
+  // columns are dealt out cyclically, so every CTA keeps about the same
+  // number of active columns as the reduction moves right
+  const int nc = rank < n ? (n - rank + HC_CS - 1) / HC_CS : 0;
+  auto first_local = [&](int j0) { return j0 > rank ? (j0 - rank + HC_CS - 1) / HC_CS : 0; };
+  cplx* H = Hs[blockIdx.y];
+  cplx* Z = Zs[blockIdx.y];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int i = tid;  // this thread's row
+  const bool row = i < n;
+
+  if (row)
+    for (int jl = 0; jl < nc; ++jl) A[(size_t)jl * n + i] = H[(size_t)(rank + HC_CS * jl) * n + i];
+  cluster.sync();  // every CTA of the cluster runs before shared memory is written remotely
+
+#ifdef HC_TIMING
+  long long tph[6] = {0, 0, 0, 0, 0, 0}, tl = clock64();
+#define HC_T(q) { long long t_ = clock64(); tph[q] += t_ - tl; tl = t_; }
+#else
+#define HC_T(q)
+#endif
+  for (int k = 0; k + 2 < n; ++k) {
+    const int j0 = k + 1;
+    const int par = k & 1;
+    cplx* v = vb + par * HC_THREADS;
+    // --- the owner of column k forms the reflector and sends it everywhere
+    if (k % HC_CS == rank) {
+      cplx* col = A + (size_t)(k / HC_CS) * n;
+      const cplx a = (row && i > j0) ? col[i] : mk(0.0, 0.0);
+      const double xn = block_sum(mk(cabs2(a), 0.0), s_red).x;
+      if (tid == 0) {
+        double beta;
+        cplx tau, scale;
+        householder(col[j0], xn, &beta, &tau, &scale);
+        col[j0] = mk(beta, 0.0);
+        s_scale = scale;
+        for (int r = 0; r < HC_CS; ++r) cluster.map_shared_rank(taus, r)[k] = tau;
+      }
+      __syncthreads();
+      cplx vi = mk(0.0, 0.0);
+      if (row && i == j0) vi = mk(1.0, 0.0);
+      if (row && i > j0) {
+        vi = cmul(a, s_scale);
+        col[i] = vi;  // kept below the subdiagonal for Q
+      }
+      if (row && i >= j0)
+        for (int r = 0; r < HC_CS; ++r) cluster.map_shared_rank(v, r)[i] = vi;
+    }
+    HC_T(0)
+    cluster.sync();  // reflector k visible in every CTA
+    HC_T(1)
+    const cplx tau = taus[k];
+    if (tau.x == 0.0 && tau.y == 0.0) continue;  // the same decision in every CTA
+    const cplx vi = (row && i >= j0) ? v[i] : mk(0.0, 0.0);
+    const int jl0 = first_local(j0);
+    // --- partial y = A[:, J_own] v_own (thread per row) ...
+    cplx ya = mk(0.0, 0.0), yb = mk(0.0, 0.0);
+    if (row) {
+      int jl = jl0;
+      for (; jl + 1 < nc; jl += 2) {
+        ya = cfma(A[(size_t)jl * n + i], v[rank + HC_CS * jl], ya);
+        yb = cfma(A[(size_t)(jl + 1) * n + i], v[rank + HC_CS * (jl + 1)], yb);
+      }
+      if (jl < nc) ya = cfma(A[(size_t)jl * n + i], v[rank + HC_CS * jl], ya);
+    }
+    const cplx yi = cadd(ya, yb);
+    if (row)
+      for (int r = 0; r < HC_CS; ++r) cluster.map_shared_rank(yp, r)[(par * HC_CS + rank) * HC_THREADS + i] = yi;
+    // ... and u_j = v^H A[J, j] (warp per column)
+    for (int jl = jl0 + warp; jl < nc; jl += HC_WARPS) {
+      const cplx* col = A + (size_t)jl * n;
+      cplx pu = mk(0.0, 0.0);
+      for (int r = j0 + lane; r < n; r += 32) pu = cadd(pu, cmulc(v[r], col[r]));
+      pu = warp_sum_c(pu);
+      if (lane == 0) us[jl] = pu;
+    }
+    HC_T(2)
+    cluster.sync();  // all partial y delivered
+    HC_T(3)
+    cplx y = mk(0.0, 0.0);
+    if (row) {
+#pragma unroll
+      for (int r = 0; r < HC_CS; ++r) y = cadd(y, yp[(par * HC_CS + r) * HC_THREADS + i]);
+    }
+    const cplx s = block_sum((row && i >= j0) ? cmulc(vi, y) : mk(0.0, 0.0), s_red);
+    // per-column coefficients of the rank-2 update: a_j = tau conj(v_j),
+    // b_j = conj(tau) z_j with z_j = u_j - tau s conj(v_j)
+    const cplx ts = cmul(tau, s), tauc = cconj(tau);
+    for (int jl = jl0 + tid; jl < nc; jl += HC_THREADS) {
+      const cplx vjc = cconj(v[rank + HC_CS * jl]);
+      ca[jl] = cmul(tau, vjc);
+      us[jl] = cmul(tauc, csub(us[jl], cmul(ts, vjc)));
+    }
+    __syncthreads();
+    // --- rank-2 update of this CTA's columns of J (thread per row)
+    if (row) {
+      const cplx vt = (i >= j0) ? vi : mk(0.0, 0.0);
+#pragma unroll 4
+      for (int jl = jl0; jl < nc; ++jl) {
+        cplx* p = A + (size_t)jl * n + i;
+        *p = csub(csub(*p, cmul(y, ca[jl])), cmul(vt, us[jl]));
+      }
+    }
+    __syncthreads();
+    HC_T(4)
+  }
+#ifdef HC_TIMING
+  if (tid == 0 && blockIdx.y == 0)
+    printf("hc rank %d: owner %lld sync1 %lld yu %lld sync2 %lld update %lld\n", rank, tph[0], tph[1], tph[2],
+           tph[3], tph[4]);
+#endif
+
+  // --- write back (reflectors below the subdiagonal), then accumulate Q
+  if (row)
+    for (int jl = 0; jl < nc; ++jl) H[(size_t)(rank + HC_CS * jl) * n + i] = A[(size_t)jl * n + i];
+  __threadfence();
+  cluster.sync();  // every column of H, with its reflector, is in global memory
+  if (row)
+    for (int jl = 0; jl < nc; ++jl) A[(size_t)jl * n + i] = mk(i == rank + HC_CS * jl ? 1.0 : 0.0, 0.0);
+  // v of column k, prefetched one step ahead into a register per row
+  auto fetch = [&](int k) -> cplx {
+    if (k < 0 || !row) return mk(0.0, 0.0);
+    if (i == k + 1) return mk(1.0, 0.0);
+    return i > k + 1 ? H[(size_t)k * n + i] : mk(0.0, 0.0);
+  };
+  cplx vnext = fetch(n - 3);
+  for (int k = n - 3; k >= 0; --k) {
+    const int j0 = k + 1;
+    cplx* v = vb + (k & 1) * HC_THREADS;
+    if (row) v[i] = vnext;
+    vnext = fetch(k - 1);
+    __syncthreads();
+    const cplx tau = taus[k];
+    if (tau.x == 0.0 && tau.y == 0.0) continue;
+    // Z[J, j] -= tau v (v^H Z[J, j]) for own columns j in J (the others are
+    // still identity columns there)
+    for (int jl = first_local(j0) + warp; jl < nc; jl += HC_WARPS) {
+      cplx* col = A + (size_t)jl * n;
+      cplx wp = mk(0.0, 0.0);
+      for (int r = j0 + lane; r < n; r += 32) wp = cadd(wp, cmulc(v[r], col[r]));
+      wp = warp_sum_c(wp);
+      const cplx tw = cmul(tau, wp);
+      for (int r = j0 + lane; r < n; r += 32) col[r] = csub(col[r], cmul(v[r], tw));
+    }
+  }
+  __syncthreads();
+  if (row)
+    for (int jl = 0; jl < nc; ++jl) Z[(size_t)(rank + HC_CS * jl) * n + i] = A[(size_t)jl * n + i];
+  cluster.sync();  // no CTA still reads reflectors from H
+  if (row)
+    for (int jl = 0; jl < nc; ++jl) {
+      const int c = rank + HC_CS * jl;
+      if (i > c + 1) H[(size_t)c * n + i] = mk(0.0, 0.0);
+    }
+}
+
+}  // namespace
+
+bool hessenberg_cluster_fits(int n) { return n >= 3 && n <= HC_THREADS && hc_layout(n).total <= 227 * 1024; }
+
+void hessenberg_cluster_batched(cplx* const* d_H, cplx* const* d_Z, int batch, int n, cudaStream_t st) {
+  if (batch <= 0) return;
+  const size_t smem = hc_layout(n).total;
+  static size_t configured = 0;
+  if (smem > configured) {
+    VRC_CUDA_CHECK(
+        cudaFuncSetAttribute(hess_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    configured = smem;
+  }
+  for (int b0 = 0; b0 < batch; b0 += 65535) {
+    const int nb = min(65535, batch - b0);
+    hess_cluster_kernel<<<dim3(HC_CS, nb), HC_THREADS, smem, st>>>(d_H + b0, d_Z + b0, n);
+  }
+  VRC_CUDA_CHECK(cudaGetLastError());
+}
+
+}  // namespace vrc

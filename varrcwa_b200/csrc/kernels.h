@@ -24,6 +24,10 @@ void zinv_batched(cplx* const* d_mats, int batch, int n, int* d_status, cudaStre
 
 // ---- eigensolver ---------------------------------------------------------------
 void hessenberg_batched(cplx* const* d_H, cplx* const* d_Z, int batch, int n, cudaStream_t st);
+// The same reduction by one cluster of CTAs per matrix with the matrix in
+// distributed shared memory (hessenberg.cu); for n where it fits.
+bool hessenberg_cluster_fits(int n);
+void hessenberg_cluster_batched(cplx* const* d_H, cplx* const* d_Z, int batch, int n, cudaStream_t st);
 // Complex Schur form + Schur vectors.  d_logs: one rotation-log buffer of
 // schur_log_bytes(n) bytes per matrix (device scratch, contents overwritten).
 // parts: SCHUR_ITERATE (QR sweeps on the active windows, rotations logged),
