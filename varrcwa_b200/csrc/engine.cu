@@ -262,8 +262,29 @@ void Engine::inverse(const std::vector<cplx*>& mats, int n, std::vector<int>* st
   }
   {
     const double nn3 = (double)n * n * n;
-    Prof pr(*this, "zinv", 8.0 * nn3 * mats.size(), 32.0 * n * (double)n * mats.size());
-    zinv_batched(dm, (int)mats.size(), n, dst, stream_);
+    const int W = zinv_blocked_width(n);
+    if (n >= 2 * W && !std::getenv("VRC_ZINV_SINGLE_CTA")) {
+      // blocked: rank-W updates on the tensor cores, in chunks of a fixed
+      // number of matrices so that the scratch block is reused
+      const size_t per = zinv_blocked_scratch(n);
+      const size_t CH = 512;
+      char* scr = (char*)bytes(CH * per);
+      for (size_t c0 = 0; c0 < mats.size(); c0 += CH) {
+        const size_t B = std::min(CH, mats.size() - c0);
+        std::vector<GemmDesc> g(B);
+        for (size_t b = 0; b < B; ++b) {
+          cplx* Mb = (cplx*)(scr + b * per);
+          g[b] = {Mb, Mb + (size_t)n * W, mats[c0 + b], mats[c0 + b], nullptr, nullptr};
+        }
+        const GemmDesc* dd = upload(g);
+        Prof pr(*this, "zinv", 8.0 * nn3 * B, 48.0 * n * (double)n * B * ((n + W - 1) / W));
+        zinv_blocked_batched(dm + c0, (int)B, n, dst ? dst + c0 : nullptr, scr, dd, stream_);
+      }
+      free_bytes(scr, CH * per);
+    } else {
+      Prof pr(*this, "zinv", 8.0 * nn3 * mats.size(), 32.0 * n * (double)n * mats.size());
+      zinv_batched(dm, (int)mats.size(), n, dst, stream_);
+    }
   }
   if (status) {
     std::vector<int> h(mats.size());

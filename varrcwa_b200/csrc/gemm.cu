@@ -2,8 +2,10 @@
 //
 //   C = diag(rs) * (alpha * A * B) * diag(cs) + beta * Cin + delta * I
 //
-// for square column-major n x n operands (every contraction of the hot path
-// is square: projections, star products, perturbation terms, P*Q).  One CTA
+// for column-major n x n operands (every contraction of the hot path is
+// square: projections, star products, perturbation terms, P*Q), or with an
+// inner dimension kdim != n (A is n x kdim, B is kdim x n) for the rank-kdim
+// updates of the blocked inversion.  One CTA
 // computes a 64 x 64 complex tile; operands are staged through shared memory
 // by 16-byte cp.async copies in a 3-stage pipeline.  The complex product
 // uses three real products (P1 = Ar Br, P2 = Ai Bi, P3 = (Ar+Ai)(Br+Bi);
@@ -43,7 +45,7 @@ __device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, doubl
 }
 
 __global__ void __launch_bounds__(NTHREADS, 2)
-    zgemm_kernel(const GemmDesc* __restrict__ descs, int n, cplx alpha, cplx beta, double delta) {
+    zgemm_kernel(const GemmDesc* __restrict__ descs, int n, int kdim, cplx alpha, cplx beta, double delta) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx* As = reinterpret_cast<cplx*>(smem_raw);        // [STAGES][BK][LDA]
   cplx* Bs = As + STAGES * BK * LDA;                    // [STAGES][BK][LDB]
@@ -59,7 +61,7 @@ __global__ void __launch_bounds__(NTHREADS, 2)
 
   const cplx* __restrict__ A = d.A;
   const cplx* __restrict__ B = d.B;
-  const int KT = (n + BK - 1) / BK;
+  const int KT = (kdim + BK - 1) / BK;
 
   auto load_tile = [&](int stage, int kt) {
     const int k0 = kt * BK;
@@ -71,13 +73,13 @@ __global__ void __launch_bounds__(NTHREADS, 2)
       // A tile: 64 rows x 8 cols, consecutive threads -> consecutive rows.
       int r = idx & 63, k = idx >> 6;
       int gr = m0 + r, gk = k0 + k;
-      bool va = (gr < n) && (gk < n);
+      bool va = (gr < n) && (gk < kdim);
       cp_async16(as + k * LDA + r, va ? (const void*)(A + (size_t)gk * n + gr) : (const void*)A, va);
       // B tile: 8 rows x 64 cols, consecutive threads -> consecutive k.
       int kb = idx & 7, c = idx >> 3;
       int gkb = k0 + kb, gc = n0 + c;
-      bool vb = (gkb < n) && (gc < n);
-      cp_async16(bs + kb * LDB + c, vb ? (const void*)(B + (size_t)gc * n + gkb) : (const void*)B, vb);
+      bool vb = (gkb < kdim) && (gc < n);
+      cp_async16(bs + kb * LDB + c, vb ? (const void*)(B + (size_t)gc * kdim + gkb) : (const void*)B, vb);
     }
   };
 
@@ -153,7 +155,8 @@ __global__ void __launch_bounds__(NTHREADS, 2)
 }  // namespace
 
 void zgemm_batched(const GemmDesc* d_descs, int batch, int n, cplx alpha, cplx beta, double delta,
-                   cudaStream_t stream) {
+                   cudaStream_t stream, int kdim) {
+  if (kdim < 0) kdim = n;
   static bool configured = false;
   if (!configured) {
     VRC_CUDA_CHECK(cudaFuncSetAttribute(zgemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -165,7 +168,7 @@ void zgemm_batched(const GemmDesc* d_descs, int batch, int n, cplx alpha, cplx b
   for (int b0 = 0; b0 < batch; b0 += 65535) {
     int nb = batch - b0 < 65535 ? batch - b0 : 65535;
     dim3 grid(tiles, nb);
-    zgemm_kernel<<<grid, NTHREADS, SMEM_BYTES, stream>>>(d_descs + b0, n, alpha, beta, delta);
+    zgemm_kernel<<<grid, NTHREADS, SMEM_BYTES, stream>>>(d_descs + b0, n, kdim, alpha, beta, delta);
   }
   VRC_CUDA_CHECK(cudaGetLastError());
 }

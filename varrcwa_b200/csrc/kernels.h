@@ -16,11 +16,19 @@ struct GemmDesc {
   const cplx* cs;   // optional column scale (n)
 };
 void zgemm_batched(const GemmDesc* d_descs, int batch, int n, cplx alpha, cplx beta, double delta,
-                   cudaStream_t stream);
+                   cudaStream_t stream, int kdim = -1);  // kdim < 0: n
 
 // ---- inverse (in place) -------------------------------------------------------
 int zinv_panel_width(int n);
 void zinv_batched(cplx* const* d_mats, int batch, int n, int* d_status, cudaStream_t stream);
+// Blocked inversion with the rank-w updates as tensor-core GEMMs.  scratch:
+// zinv_blocked_scratch(n) bytes per matrix; d_descs[b] = {M_b, M_b + n W,
+// mat_b, mat_b} with M_b = scratch + b * zinv_blocked_scratch(n) and
+// W = zinv_blocked_width(n).
+int zinv_blocked_width(int n);
+size_t zinv_blocked_scratch(int n);
+void zinv_blocked_batched(cplx* const* d_mats, int batch, int n, int* d_status, void* scratch,
+                          const GemmDesc* d_descs, cudaStream_t stream);
 
 // ---- eigensolver ---------------------------------------------------------------
 void hessenberg_batched(cplx* const* d_H, cplx* const* d_Z, int batch, int n, cudaStream_t st);
