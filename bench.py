@@ -40,7 +40,7 @@ def parse():
     p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--batch", type=int, default=64, help="cells per step per GPU")
+    p.add_argument("--batch", type=int, default=128, help="cells per step per GPU")
     p.add_argument("--workload", default="c2", choices=["c2", "c3"])
     p.add_argument("--pe", type=float, default=1e-2)
     p.add_argument("--npix", type=int, default=256)
@@ -198,6 +198,28 @@ def run_reference(a, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def profiled_traffic(family, flops_per_launch):
+    """DRAM bytes (read + write) per average launch of the family's main
+    kernel, from the committed ncu summary profiles/<family>_traffic.txt
+    (`bytes_per_matrix` measured on a smaller launch of the same kernel,
+    scaled by the matrices per launch = flops per launch / `flops_per_matrix`),
+    or None when no capture is summarised."""
+    p = ROOT / "profiles" / f"{family}_traffic.txt"
+    if not p.exists() or not flops_per_launch:
+        return None
+    kv = {}
+    for ln in p.read_text().splitlines():
+        parts = ln.split()
+        if len(parts) == 2:
+            try:
+                kv[parts[0]] = float(parts[1])
+            except ValueError:
+                pass
+    if "bytes_per_matrix" not in kv or "flops_per_matrix" not in kv:
+        return None
+    return kv["bytes_per_matrix"] * flops_per_launch / kv["flops_per_matrix"]
+
+
 def metric_name():
     return "batched S-matrix solves/s (FP64 varRCWA forward, per-order T/R)"
 
@@ -266,21 +288,29 @@ def run_ours(a, rank, world, local_rank):
     m = 121 if a.workload == "c2" else None
     h2d = sum(len(np.asarray(d.get("eps", [])).tobytes()) for d in descs) + 256 * len(descs)
     d2h = sum(2 * 2 * d["nx"] * d["ny"] * 8 for d in descs)
-    # dominant kernel family and its roofline
+    # dominant kernel family and its roofline.  FP64 work on B200 runs either
+    # on the DMMA tensor pipe (GEMMs, the inversion's rank-32 updates) or on
+    # the FP64 FMA pipe (Hessenberg, QR, back substitution); the two peaks
+    # coincide on this part, so both are measured against cuBLAS DGEMM.
     fam = max(stats.items(), key=lambda kv: kv[1]["ms"])
     hbm_peak, hbm_src = measured_peaks()
     name, f = fam
-    if f["flops"] > 0 and name in ("zgemm", "zinv", "hessenberg", "schur_qr", "trevc"):
+    limiter = {"zgemm": "FP64 DMMA tensor pipe", "zinv": "panel reduction (latency) + DMMA rank-32 updates",
+               "hessenberg": "cluster barriers per column (latency)",
+               "schur_qr": "sequential bulge chase (latency)", "schur_replay": "FP64 pipe / memory latency",
+               "trevc": "sequential back substitution (latency)"}.get(name, "HBM bandwidth")
+    traffic = profiled_traffic(name, f["flops"] / max(f["launches"], 1))
+    if f["flops"] > 0:
         achieved = f["flops"] / (f["ms"] * 1e-3) / 1e12
         roof = {"kernel": name, "bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                 "frac": achieved / fp64_peak if fp64_peak else None,
-                "peak_source": "measured cuBLAS DGEMM (FP64 DMMA) on this GPU, 8192^3",
-                "avg_launch_ms": f["ms"] / max(f["launches"], 1), "traffic": None}
+                "peak_source": "measured cuBLAS DGEMM (FP64) on this GPU, 8192^3, in this run",
+                "limiter": limiter, "avg_launch_ms": f["ms"] / max(f["launches"], 1), "traffic": traffic}
     else:
         achieved = f["bytes"] / (f["ms"] * 1e-3) / 1e9
         roof = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                 "frac": achieved / hbm_peak, "peak_source": f"{hbm_src} MEASURED_PEAKS.json hbm_gbs",
-                "avg_launch_ms": f["ms"] / max(f["launches"], 1), "traffic": None}
+                "limiter": limiter, "avg_launch_ms": f["ms"] / max(f["launches"], 1), "traffic": traffic}
     gemm = stats.get("zgemm")
     breakdown = {k: {"ms": round(v["ms"], 3), "share": round(v["ms"] / sum(x["ms"] for x in stats.values()), 4),
                      "launches": v["launches"],

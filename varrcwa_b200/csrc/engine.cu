@@ -804,10 +804,13 @@ void Engine::eig(std::vector<EigReq>& reqs, int n, std::vector<int>* status) {
       cplx* const* dL = upload(lam);
       void* const* dG = upload(logs);
       {
-        Prof pr(*this, "schur_qr", 80.0 * nn3 * B, 4.0 * mbytes * B);
+        // nominal LAPACK count for the complex Schur form with vectors (~80 n^3
+        // real), half for T's active windows, half for the replay onto Z and
+        // the rest of T
+        Prof pr(*this, "schur_qr", 40.0 * nn3 * B, 4.0 * mbytes * B);
         schur_batched(dH, dZ, dL, dG, (int)B, n, dstat, stream_, SCHUR_ITERATE);
       }
-      Prof pr(*this, "schur_replay", 0.0, 4.0 * mbytes * B, 2);
+      Prof pr(*this, "schur_replay", 40.0 * nn3 * B, 4.0 * mbytes * B, 2);
       schur_batched(dH, dZ, dL, dG, (int)B, n, dstat, stream_, SCHUR_REPLAY);
     }
     if (std::getenv("VRC_QR_STATS")) {
