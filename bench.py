@@ -46,6 +46,8 @@ def parse():
     p.add_argument("--npix", type=int, default=256)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-cells", type=int, default=1, help="cells in the bounded CPU sample")
+    p.add_argument("--plain-cells", type=int, default=8,
+                   help="cells timed one per call (the plain per-solve form of the metric); 0 skips")
     return p.parse_args()
 
 
@@ -328,6 +330,19 @@ def run_ours(a, rank, world, local_rank):
     if gemm:
         line["zgemm_tflops"] = gemm["flops"] / (gemm["ms"] * 1e-3) / 1e12
         line["fp64_dgemm_peak_tflops"] = fp64_peak
+    # the plain form the metric compares against: the same cells submitted
+    # one structure per call on the same GPU (outside the timed region)
+    if world == 1 and a.plain_cells > 0:
+        torch.cuda.synchronize()
+        tp = time.perf_counter()
+        for d in descs[: a.plain_cells]:
+            ctx.order_powers([d], method="redheffer", pe=a.pe, side=1)
+        torch.cuda.synchronize()
+        tpl = time.perf_counter() - tp
+        plain = min(a.plain_cells, len(descs)) / tpl
+        line["plain_per_solve"] = {"value": plain, "unit": "solves/s", "cells": min(a.plain_cells, len(descs)),
+                                   "form": "one cell per C-ABI call, same GPU, host buffers"}
+        line["batched_over_plain"] = e2e / plain
     if world == 1 and not a.no_cpu_baseline:
         sample = descs[: a.cpu_cells]
         dt = cpu_sample(sample, a.pe)
