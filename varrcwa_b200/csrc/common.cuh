@@ -42,6 +42,16 @@ __device__ __forceinline__ cplx cdiv(cplx a, cplx b) {
   }
 }
 __device__ __forceinline__ cplx cinv(cplx b) { return cdiv(mk(1.0, 0.0), b); }
+// 1 / b as conj(b) / |b|^2 with one real reciprocal, for |b| well inside the
+// double range (no intermediate over- or underflow); Smith's form otherwise.
+__device__ __forceinline__ cplx cinv_fast(cplx b) {
+  const double m = fmax(fabs(b.x), fabs(b.y));
+  if (m > 1e-150 && m < 1e150) {
+    const double r = 1.0 / (b.x * b.x + b.y * b.y);
+    return mk(b.x * r, -b.y * r);
+  }
+  return cinv(b);
+}
 __device__ __forceinline__ cplx cexp_i(cplx g, double t) {
   // exp(i * g * t)
   double re = -g.y * t, im = g.x * t;

@@ -824,6 +824,29 @@ void Engine::eig(std::vector<EigReq>& reqs, int n, std::vector<int>* status) {
         sync();
         for (int q = 0; q < 4; ++q) tot[q] += hh[q], tot[4 + q] += (double)tt[q];
       }
+      {
+        // sweep-size profile of the first matrix: rounds spent in sweeps on
+        // windows of each size class
+        int hh[4];
+        VRC_CUDA_CHECK(cudaMemcpyAsync(hh, logs[0], sizeof(hh), cudaMemcpyDeviceToHost, stream_));
+        sync();
+        std::vector<int> rec((size_t)hh[0] * 8);
+        if (hh[0] > 0)
+          VRC_CUDA_CHECK(cudaMemcpyAsync(rec.data(), (char*)logs[0] + 64, rec.size() * sizeof(int),
+                                         cudaMemcpyDeviceToHost, stream_));
+        sync();
+        double cls[6] = {0, 0, 0, 0, 0, 0};
+        int cnt[6] = {0, 0, 0, 0, 0, 0};
+        for (int q = 0; q < hh[0]; ++q) {
+          const int w = rec[q * 8 + 1] - rec[q * 8] + 1, R = rec[q * 8 + 3];
+          const int c = w <= 8 ? 0 : w <= 16 ? 1 : w <= 32 ? 2 : w <= 64 ? 3 : w <= 128 ? 4 : 5;
+          cls[c] += R;
+          cnt[c] += 1;
+        }
+        fprintf(stderr, "[vrc qr] first matrix: window<=8: %d sweeps %.0f rounds; <=16: %d %.0f; <=32: %d %.0f; "
+                        "<=64: %d %.0f; <=128: %d %.0f; >128: %d %.0f\n",
+                cnt[0], cls[0], cnt[1], cls[1], cnt[2], cls[2], cnt[3], cls[3], cnt[4], cls[4], cnt[5], cls[5]);
+      }
       fprintf(stderr,
               "[vrc qr] n=%d matrices=%zu per matrix: sweeps=%.1f rounds=%.0f rotation slots=%.0f (%.2f n^2) "
               "Mcycles defl=%.2f shift=%.2f rounds=%.2f far=%.2f\n",

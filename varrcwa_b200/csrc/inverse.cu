@@ -11,6 +11,8 @@
 // applied to every other column as one rank-nb update
 //     a[:, j] <- P a[:, j];  a[:, j] += (Tp - E) a[k:k+nb, j]
 // so the matrix is streamed once per panel instead of once per pivot.
+#include <cstdlib>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -305,6 +307,188 @@ __global__ void __launch_bounds__(PANEL_THREADS)
   if (tid == 0 && status && s_bad) status[blockIdx.x] = ST_ESINGULAR;
 }
 
+// The same panel step with the panel held in registers (n <= 256): thread
+// (h, i) of 512 keeps row i of panel columns [16h, 16h+16); per pivot only
+// the pivot candidates, the exchanged rows, the multipliers and the scaled
+// pivot row pass through shared memory.
+constexpr int RPN_THREADS = 512;
+constexpr int RPN_STAGE = 32 * 1024;  // bytes for the row moves of the other columns
+
+__global__ void __launch_bounds__(RPN_THREADS, 1)
+    zinv_panel_reg_kernel(cplx* const* __restrict__ mats, cplx* __restrict__ scratch, size_t per, int n, int k,
+                          int w, int W, int* __restrict__ status) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx* stage = reinterpret_cast<cplx*>(smem_raw);                 // [RPN_STAGE bytes]
+  int* src = reinterpret_cast<int*>(smem_raw + RPN_STAGE);         // [256]
+  int* rows = src + 256;                                           // [64]
+  __shared__ PivotCand red[8];
+  __shared__ cplx prow[32];
+  __shared__ cplx fcol[256];
+  __shared__ int s_bad, s_nrows;
+
+  cplx* a = mats[blockIdx.x];
+  cplx* M = scratch + (size_t)blockIdx.x * per;
+  cplx* X = M + (size_t)n * W;
+  int* piv = reinterpret_cast<int*>(M + 2 * (size_t)n * W);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int h = tid >> 8, i = tid & 255;
+  const bool row = i < n;
+
+#ifdef ZP_TIMING
+  long long zt0 = clock64(), zt1 = 0, zt2 = 0, zt3 = 0, zt4 = 0, zs[4] = {0, 0, 0, 0};
+#endif
+  cplx r[16];
+#pragma unroll
+  for (int c = 0; c < 16; ++c) {
+    const int gc = 16 * h + c;
+    r[c] = (row && gc < w) ? a[(size_t)(k + gc) * n + i] : mk(0.0, 0.0);
+  }
+  for (int q = tid; q < n; q += RPN_THREADS) src[q] = q;
+  if (tid == 0) {
+    s_bad = 0;
+    s_nrows = 0;
+  }
+  // Rows stay in their threads; the interchanges only relabel them: lpos is
+  // the row index this thread's row has after the interchanges so far.
+  int lpos = i;
+  __syncthreads();
+#ifdef ZP_TIMING
+  zt1 = clock64();
+#endif
+  // the step loop is not unrolled (its body is large); a thread's entry of
+  // column s is picked from the register row by an unrolled select
+  auto pick = [&](int cs) {
+    cplx v = r[0];
+#pragma unroll
+    for (int c = 1; c < 16; ++c)
+      if (c == cs) v = r[c];
+    return v;
+  };
+#pragma unroll 1
+  for (int s = 0; s < 32; ++s) {
+    if (s < w) {
+      const int r0 = k + s;
+      const int hs = s >> 4, cs = s & 15;
+      if (h == hs) {
+        PivotCand c{-1.0, n};
+        if (row && lpos >= r0) {
+          c.v = cabs1(pick(cs));
+          c.i = lpos;
+        }
+        c = warp_argmax(c);
+        if (lane == 0) red[warp & 7] = c;
+      }
+#ifdef ZP_TIMING
+      long long ta = clock64();
+#endif
+      __syncthreads();
+#ifdef ZP_TIMING
+      long long tb = clock64();
+      zs[0] += tb - ta;
+#endif
+      // every thread reduces the eight candidates itself (same order, same result)
+      PivotCand cc = red[0];
+#pragma unroll
+      for (int q = 1; q < 8; ++q) {
+        const PivotCand o = red[q];
+        if (o.v > cc.v || (o.v == cc.v && o.i < cc.i)) cc = o;
+      }
+      const bool bad = !(cc.v > 0.0) || !isfinite(cc.v) || cc.i >= n;
+      const int p = bad ? r0 : cc.i;
+      if (tid == 0) {
+        if (bad) s_bad = 1;
+        piv[r0] = p;
+        const int t = src[r0];
+        src[r0] = src[p];
+        src[p] = t;
+      }
+      if (lpos == p) lpos = r0;
+      else if (lpos == r0) lpos = p;
+      // the pivot row (now labelled r0) and the multipliers of column s
+      const bool prow_thread = row && lpos == r0;
+      if (prow_thread) {
+#pragma unroll
+        for (int c = 0; c < 16; ++c) prow[16 * h + c] = r[c];
+      }
+      if (h == hs && row) fcol[i] = pick(cs);
+#ifdef ZP_TIMING
+      long long tc = clock64();
+      zs[1] += tc - tb;
+#endif
+      __syncthreads();
+#ifdef ZP_TIMING
+      long long td = clock64();
+      zs[2] += td - tc;
+#endif
+      const cplx ip = bad ? mk(1.0, 0.0) : cinv_fast(prow[s]);
+      if (prow_thread) {
+#pragma unroll
+        for (int c = 0; c < 16; ++c) {
+          const int gc = 16 * h + c;
+          r[c] = cmul(gc == s ? mk(1.0, 0.0) : r[c], ip);
+        }
+      } else if (row) {
+        const cplx f = cmul(fcol[i], ip);
+#pragma unroll
+        for (int c = 0; c < 16; ++c) {
+          const int gc = 16 * h + c;
+          // column s: -a(i, s) / pivot; others: a(i, c) - a(i, s) / pivot * a(r0, c)
+          if (gc < w) r[c] = (gc == s) ? cneg(f) : csub(r[c], cmul(f, prow[gc]));
+        }
+      }
+#ifdef ZP_TIMING
+      zs[3] += clock64() - td;
+#endif
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 16; ++c) {
+    const int gc = 16 * h + c;
+    if (row && gc < w) {
+      const cplx v = r[c];
+      a[(size_t)(k + gc) * n + lpos] = v;
+      M[(size_t)gc * n + lpos] = (lpos == k + gc) ? mk(v.x - 1.0, v.y) : v;
+    }
+  }
+#ifdef ZP_TIMING
+  zt2 = clock64();
+#endif
+  for (int q = tid; q < n; q += RPN_THREADS)
+    if (src[q] != q) rows[atomicAdd(&s_nrows, 1)] = q;
+  __syncthreads();
+  const int nrows = s_nrows;
+  constexpr int nwarps = RPN_THREADS / 32;
+  const int cw = max(1, (int)(RPN_STAGE / 16 / max(nrows, 1)));
+  for (int g0 = 0; g0 < n && nrows > 0; g0 += cw) {
+    const int g1 = min(n, g0 + cw);
+    for (int j = g0 + warp; j < g1; j += nwarps) {
+      if (j >= k && j < k + w) continue;
+      for (int q = lane; q < nrows; q += 32) stage[(size_t)(j - g0) * nrows + q] = a[(size_t)j * n + src[rows[q]]];
+    }
+    __syncthreads();
+    for (int j = g0 + warp; j < g1; j += nwarps) {
+      if (j >= k && j < k + w) continue;
+      for (int q = lane; q < nrows; q += 32) a[(size_t)j * n + rows[q]] = stage[(size_t)(j - g0) * nrows + q];
+    }
+    __syncthreads();
+  }
+#ifdef ZP_TIMING
+  zt3 = clock64();
+#endif
+  for (int j = warp; j < n; j += nwarps) {
+    const bool pc = j >= k && j < k + w;
+    for (int s2 = lane; s2 < w; s2 += 32) X[(size_t)j * w + s2] = pc ? mk(0.0, 0.0) : a[(size_t)j * n + k + s2];
+  }
+  if (tid == 0 && status && s_bad) status[blockIdx.x] = ST_ESINGULAR;
+#ifdef ZP_TIMING
+  __syncthreads();
+  zt4 = clock64();
+  if (tid == 0 && blockIdx.x == 0)
+    printf("zp k=%d load %lld pivots %lld [sync1 %lld reduce %lld sync2 %lld elim %lld] permute %lld extract %lld\n", k,
+           zt1 - zt0, zt2 - zt1, zs[0], zs[1], zs[2], zs[3], zt3 - zt2, zt4 - zt3);
+#endif
+}
+
 __global__ void __launch_bounds__(256)
     zinv_colswap_kernel(cplx* const* __restrict__ mats, const cplx* __restrict__ scratch, size_t per, int n, int w) {
   cplx* a = mats[blockIdx.x];
@@ -352,13 +536,26 @@ void zinv_blocked_batched(cplx* const* d_mats, int batch, int n, int* d_status, 
     VRC_CUDA_CHECK(cudaFuncSetAttribute(zinv_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     configured = smem;
   }
+  // registers hold the panel when every row has a thread of each half
+  const bool use_reg = n <= 256 && W == 32 && !std::getenv("VRC_ZINV_SMEM_PANEL");
+  const size_t reg_smem = RPN_STAGE + (256 + 64) * sizeof(int);
+  static bool reg_configured = false;
+  if (use_reg && !reg_configured) {
+    VRC_CUDA_CHECK(
+        cudaFuncSetAttribute(zinv_panel_reg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)reg_smem));
+    reg_configured = true;
+  }
   cplx* scr = static_cast<cplx*>(scratch);
   for (int b0 = 0; b0 < batch; b0 += 65535) {
     const int nb = min(65535, batch - b0);
     for (int k = 0; k < n; k += W) {
       const int w = min(W, n - k);
-      zinv_panel_kernel<<<nb, PANEL_THREADS, smem, stream>>>(d_mats + b0, scr + (size_t)b0 * per, per, n, k, w, W,
-                                                             d_status ? d_status + b0 : nullptr);
+      if (use_reg)
+        zinv_panel_reg_kernel<<<nb, RPN_THREADS, reg_smem, stream>>>(
+            d_mats + b0, scr + (size_t)b0 * per, per, n, k, w, W, d_status ? d_status + b0 : nullptr);
+      else
+        zinv_panel_kernel<<<nb, PANEL_THREADS, smem, stream>>>(d_mats + b0, scr + (size_t)b0 * per, per, n, k, w, W,
+                                                               d_status ? d_status + b0 : nullptr);
       VRC_CUDA_CHECK(cudaGetLastError());
       // descriptor b: A = M (n x w, leading dimension n), B = X (w x n,
       // leading dimension w) at M + n W, C = Cin = the matrix
