@@ -35,7 +35,10 @@ constexpr int QR_THREADS = 256;
 constexpr int NBMAX = QR_THREADS / 32;           // bulges per sweep (one warp each)
 constexpr int QB = 32;                           // rounds per chunk
 constexpr int QD = QB + 3 * (NBMAX - 1) + 3;     // diagonal window size (56)
-constexpr size_t QR_SMEM = (size_t)(QD * QD + 2 * NBMAX * QB) * sizeof(cplx);
+// leading dimension of the window: odd in 16-byte units, so that the lanes
+// of a row access (stride QLD) fall in distinct shared-memory banks
+constexpr int QLD = QD + 1;
+constexpr size_t QR_SMEM = (size_t)(QD * QLD + 2 * NBMAX * QB) * sizeof(cplx);
 
 struct QrLogHeader {
   int nsweeps, nrot;
@@ -203,8 +206,8 @@ __global__ void __launch_bounds__(QR_THREADS, 2)
     hqr_kernel(cplx* const* __restrict__ Hs, void* const* __restrict__ logs, cplx* const* __restrict__ Ws, int n,
                int sweep_cap, long long rot_cap, int* __restrict__ status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  cplx* D = reinterpret_cast<cplx*>(smem_raw);  // [QD][QD] column-major window
-  cplx* s_tau = D + QD * QD;                    // [NBMAX][QB]
+  cplx* D = reinterpret_cast<cplx*>(smem_raw);  // [QD][QLD] column-major window
+  cplx* s_tau = D + QD * QLD;                   // [NBMAX][QB]
   cplx* s_v2 = s_tau + NBMAX * QB;              // [NBMAX][QB]
   __shared__ cplx s_shift[NBMAX];
   __shared__ cplx s_small[NBMAX * NBMAX];
@@ -324,11 +327,11 @@ __global__ void __launch_bounds__(QR_THREADS, 2)
         const int dn = de - ds + 1;
         for (int idx = tid; idx < dn * dn; idx += QR_THREADS) {
           const int c = idx / dn, r = idx - c * dn;
-          D[c * QD + r] = h(ds + r, ds + c);
+          D[c * QLD + r] = h(ds + r, ds + c);
         }
         __syncthreads();
         if (s_over) break;
-        auto dd = [&](int r, int c) -> cplx& { return D[(c - ds) * QD + (r - ds)]; };
+        auto dd = [&](int r, int c) -> cplx& { return D[(c - ds) * QLD + (r - ds)]; };
         auto reflect = [&](int r) {
           const int k = m + r - 3 * a;
           if (lane == 0 && mine && k >= m && k <= i - 1) {
@@ -387,7 +390,7 @@ __global__ void __launch_bounds__(QR_THREADS, 2)
         // Write the window back and log this chunk's rotations (round-major).
         for (int idx = tid; idx < dn * dn; idx += QR_THREADS) {
           const int c = idx / dn, r = idx - c * dn;
-          h(ds + r, ds + c) = D[c * QD + r];
+          h(ds + r, ds + c) = D[c * QLD + r];
         }
         const int nr = r1 - r0;
         for (int idx = tid; idx < nb * nr; idx += QR_THREADS) {
