@@ -1,0 +1,49 @@
+"""Host-side pieces of bench.py that run without a GPU: argument defaults,
+the workload cells, the clock-record parsing, the profiled-traffic scaling
+and the JSON config block."""
+import importlib
+import sys
+
+import pytest
+
+
+@pytest.fixture(scope="module")
+def bench():
+    sys.path.insert(0, ".")
+    return importlib.import_module("bench")
+
+
+def test_defaults_and_helpers_present(bench, monkeypatch):
+    monkeypatch.setattr(sys, "argv", ["bench.py"])
+    a = bench.parse()
+    assert (a.gpus, a.impl, a.workload, a.batch) == (1, "ours", "c2", 128)
+    assert a.warmup >= 3
+    for name in ("ClockSampler", "measured_peaks", "dgemm_peak_tflops", "cpu_sample", "run_reference",
+                 "run_ours", "profiled_traffic", "workload_config", "metric_name", "make_cells"):
+        assert hasattr(bench, name), name
+
+
+def test_cells_are_seeded_and_rank_disjoint(bench):
+    c0 = bench.make_cells("c2", 3, 0, 16)
+    c1 = bench.make_cells("c2", 3, 1, 16)
+    assert len(c0) == 3 and all(d["nx"] == 11 and d["ny"] == 11 for d in c0)
+    assert bench.make_cells("c2", 3, 0, 16)[1]["r0"] == c0[1]["r0"]  # deterministic
+    assert [d["r0"] for d in c0] != [d["r0"] for d in c1]
+
+
+def test_clock_record_parsing(bench):
+    cs = bench.ClockSampler(0)
+    cs.proc = type("P", (), {"terminate": lambda s: None, "wait": lambda s, timeout=None: 0})()
+    cs.lines = ["0, 1965, 1965, 700.0, 0x0, Not Active, Not Active, Not Active, Not Active",
+                "0, 1900, 1965, 990.0, 0x4, Not Active, Not Active, Not Active, Active",
+                "0, 1965, 1965, 800.0, 0x0, Not Active, Not Active, Not Active, Not Active"]
+    clk = cs.stop()
+    assert clk["sm_mhz"] == 1965.0 and clk["sm_max_mhz"] == 1965.0
+    assert clk["reasons"] == ["sw_power_cap"] and clk["samples"] == 3
+
+
+def test_profiled_traffic_scales_by_matrices(bench):
+    per_launch_one = bench.profiled_traffic("schur_qr", 40 * 242 ** 3)
+    assert per_launch_one is not None and per_launch_one > 0
+    assert bench.profiled_traffic("schur_qr", 2 * 40 * 242 ** 3) == pytest.approx(2 * per_launch_one)
+    assert bench.profiled_traffic("no_such_family", 1.0) is None
