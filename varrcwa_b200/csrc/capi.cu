@@ -1,7 +1,10 @@
 // extern "C" boundary (include/vrc.h) over the engine.
+#include <cstdlib>
 #include "../../include/vrc.h"
 #include "engine.h"
 
+#include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -45,8 +48,28 @@ struct Timed {
   long long l0;
   explicit Timed(vrc_context* c) : ctx(c), l0(c->eng->launches) {
     VRC_CUDA_CHECK(cudaEventRecord(ctx->ev0, ctx->eng->stream()));
+    c->eng->bubble_ms_ = c->eng->sync_ms_ = 0.0;
+    c->eng->nsync_ = 0;
+    c->eng->gap_.clear();
+    c->eng->t_sync_ret_ = std::chrono::duration<double, std::milli>(
+                              std::chrono::steady_clock::now().time_since_epoch()).count();
   }
   void done() {
+    if (std::getenv("VRC_HOST_STATS"))
+    {
+      ctx->eng->sync();
+      fprintf(stderr, "[vrc host] syncs %lld, blocked %.1f ms, host gaps before the next launch %.1f ms\n",
+              ctx->eng->nsync_, ctx->eng->sync_ms_, ctx->eng->bubble_ms_);
+      std::vector<std::pair<double, std::string>> g;
+      double tot = 0.0;
+      for (auto& kv : ctx->eng->gap_) {
+        g.push_back({kv.second, kv.first});
+        tot += kv.second;
+      }
+      std::sort(g.rbegin(), g.rend());
+      fprintf(stderr, "[vrc host] GPU gaps between profiled families: %.1f ms total\n", tot);
+      for (size_t q = 0; q < g.size() && q < 12; ++q) fprintf(stderr, "  %8.1f ms  %s\n", g[q].first, g[q].second.c_str());
+    }
     VRC_CUDA_CHECK(cudaEventRecord(ctx->ev1, ctx->eng->stream()));
     VRC_CUDA_CHECK(cudaEventSynchronize(ctx->ev1));
     float ms = 0.f;

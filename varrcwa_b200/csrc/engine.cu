@@ -117,8 +117,16 @@ Engine::~Engine() {
   if (own_stream_) cudaStreamDestroy(stream_);
 }
 
+static double host_now_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
 void Engine::sync() {
+  const double t0 = host_now_ms();
   VRC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+  t_sync_ret_ = host_now_ms();
+  sync_ms_ += t_sync_ret_ - t0;
+  ++nsync_;
   stage_off_ = 0;
   if (!pend_prof_.empty()) resolve_prof();
 }
@@ -143,8 +151,17 @@ void Engine::resolve_prof() {
     f.launches += p.nl;
     f.flops += p.flops;
     f.bytes += p.bytes;
+    if (last_b_) {
+      // GPU time between the previous profiled family and this one (idle,
+      // or small unprofiled copies): a diagnostic of host-side bubbles
+      float gap = 0.f;
+      VRC_CUDA_CHECK(cudaEventElapsedTime(&gap, last_b_, p.a));
+      gap_[last_fam_ + " -> " + p.fam] += gap;
+      ev_pool_.push_back(last_b_);
+    }
     ev_pool_.push_back(p.a);
-    ev_pool_.push_back(p.b);
+    last_b_ = p.b;
+    last_fam_ = p.fam;
   }
   pend_prof_.clear();
 }
@@ -166,6 +183,10 @@ void Engine::reset_fam_stats() {
 
 Engine::Prof::Prof(Engine& eng, const char* f, double fl, double by, int nlaunch)
     : e(eng), fam(f), flops(fl), bytes(by), nl(nlaunch) {
+  if (e.t_sync_ret_ >= 0.0) {
+    e.bubble_ms_ += host_now_ms() - e.t_sync_ret_;
+    e.t_sync_ret_ = -1.0;
+  }
   if (e.profiling_) {
     a = e.take_event();
     VRC_CUDA_CHECK(cudaEventRecord(a, e.stream_));

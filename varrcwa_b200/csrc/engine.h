@@ -271,6 +271,16 @@ class Engine {
   void* ws_ = nullptr;
   size_t ws_cap_ = 0;
   bool profiling_ = false;
+  // host-bubble diagnostic (VRC_HOST_STATS): time from a sync's return to
+  // the next profiled launch, when the GPU has nothing queued
+ public:
+  double bubble_ms_ = 0.0, sync_ms_ = 0.0;
+  std::map<std::string, double> gap_;  // GPU gaps between consecutive profiled families
+  cudaEvent_t last_b_ = nullptr;
+  std::string last_fam_;
+  long long nsync_ = 0;
+  double t_sync_ret_ = -1.0;
+ private:
   double alloc_ms0_ = 0.0;
   struct PendingProf {
     const char* fam;
