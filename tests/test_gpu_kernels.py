@@ -35,7 +35,7 @@ def test_zinv_singular_reports_status(ctx):
     assert st[0] == 4  # VRC_ESINGULAR
 
 
-@pytest.mark.parametrize("n", [3, 20, 82, 162, 242])
+@pytest.mark.parametrize("n", [3, 20, 82, 162, 242, 338, 450])
 def test_eig_random(ctx, n):
     A = _rand(1, n)[0]
     lam, W = ctx.eig(A)

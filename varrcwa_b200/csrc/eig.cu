@@ -282,7 +282,18 @@ void launch_hess(cplx* const* H, cplx* const* Z, int batch, int n, cudaStream_t 
 
 void hessenberg_batched(cplx* const* d_H, cplx* const* d_Z, int batch, int n, cudaStream_t st) {
   if (batch <= 0) return;
-  if (hessenberg_cluster_fits(n) && !std::getenv("VRC_HESS_SINGLE_CTA")) {
+  // Cluster reduction: always for n <= 256 (matrix in shared memory); for
+  // larger n (matrix in L2) when the batch is too small to give every SM two
+  // matrices, or when n is large enough that the single-CTA reduction's
+  // per-matrix latency dominates (measured crossover between 338 and 450).
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    VRC_CUDA_CHECK(cudaGetDevice(&dev));
+    VRC_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  }
+  const bool cluster = hessenberg_cluster_fits(n) && (n <= 256 || n >= 400 || batch < 2 * sms);
+  if (cluster && !std::getenv("VRC_HESS_SINGLE_CTA")) {
     hessenberg_cluster_batched(d_H, d_Z, batch, n, st);
     return;
   }

@@ -249,12 +249,211 @@ __global__ void __cluster_dims__(HC_CS, 1, 1) __launch_bounds__(HC_THREADS, 1)
     }
 }
 
+// The same cluster reduction for 256 < n <= 512 with the matrix left in
+// global memory (L2 resident for the clusters in flight): there is not enough
+// shared memory for it.  Each CTA works in place on its own columns of H
+// (cyclic), each thread on rows tid and tid + 256; only the reflector, the
+// partial products y and the tau are exchanged, as above.  Q is accumulated
+// in place in the CTA's own columns of Z.
+constexpr int HG_RPT = 2;                     // rows per thread
+constexpr int HG_MAXN = HC_THREADS * HG_RPT;  // 512
+constexpr int HG_MAXW = (HG_MAXN + HC_CS - 1) / HC_CS;
+constexpr size_t HG_SMEM = (2 * (size_t)HG_MAXN + 2 * (size_t)HC_CS * HG_MAXN + HG_MAXN + 2 * HG_MAXW) * sizeof(cplx);
+
+__global__ void __cluster_dims__(HC_CS, 1, 1) __launch_bounds__(HC_THREADS, 1)
+    hess_cluster_global_kernel(cplx* const* __restrict__ Hs, cplx* const* __restrict__ Zs, int n) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ cplx s_red[HC_WARPS];
+  __shared__ cplx s_scale;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = (int)cluster.block_rank();
+  cplx* vb = reinterpret_cast<cplx*>(smem_raw);  // [2][HG_MAXN]
+  cplx* yp = vb + 2 * HG_MAXN;                    // [2][HC_CS][HG_MAXN]
+  cplx* taus = yp + 2 * HC_CS * HG_MAXN;          // [HG_MAXN]
+  cplx* us = taus + HG_MAXN;                      // [HG_MAXW]
+  cplx* ca = us + HG_MAXW;                        // [HG_MAXW]
+
+  const int nc = rank < n ? (n - rank + HC_CS - 1) / HC_CS : 0;
+  auto first_local = [&](int j0) { return j0 > rank ? (j0 - rank + HC_CS - 1) / HC_CS : 0; };
+  cplx* H = Hs[blockIdx.y];
+  cplx* Z = Zs[blockIdx.y];
+  auto colp = [&](int jl) { return H + (size_t)(rank + HC_CS * jl) * n; };
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  cluster.sync();  // every CTA of the cluster runs before shared memory is written remotely
+
+  for (int k = 0; k + 2 < n; ++k) {
+    const int j0 = k + 1;
+    const int par = k & 1;
+    cplx* v = vb + par * HG_MAXN;
+    if (k % HC_CS == rank) {
+      cplx* col = colp(k / HC_CS);
+      cplx a[HG_RPT];
+      double part = 0.0;
+#pragma unroll
+      for (int q = 0; q < HG_RPT; ++q) {
+        const int i = tid + HC_THREADS * q;
+        a[q] = (i < n && i > j0) ? col[i] : mk(0.0, 0.0);
+        part += cabs2(a[q]);
+      }
+      const double xn = block_sum(mk(part, 0.0), s_red).x;
+      if (tid == 0) {
+        double beta;
+        cplx tau, scale;
+        householder(col[j0], xn, &beta, &tau, &scale);
+        col[j0] = mk(beta, 0.0);
+        s_scale = scale;
+        for (int r = 0; r < HC_CS; ++r) cluster.map_shared_rank(taus, r)[k] = tau;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < HG_RPT; ++q) {
+        const int i = tid + HC_THREADS * q;
+        if (i >= n || i < j0) continue;
+        cplx vi = mk(1.0, 0.0);
+        if (i > j0) {
+          vi = cmul(a[q], s_scale);
+          col[i] = vi;  // kept below the subdiagonal for Q
+        }
+        for (int r = 0; r < HC_CS; ++r) cluster.map_shared_rank(v, r)[i] = vi;
+      }
+    }
+    cluster.sync();  // reflector k visible in every CTA
+    const cplx tau = taus[k];
+    if (tau.x == 0.0 && tau.y == 0.0) continue;  // the same decision in every CTA
+    const int jl0 = first_local(j0);
+    cplx vi[HG_RPT];
+#pragma unroll
+    for (int q = 0; q < HG_RPT; ++q) {
+      const int i = tid + HC_THREADS * q;
+      vi[q] = (i < n && i >= j0) ? v[i] : mk(0.0, 0.0);
+    }
+    // partial y (thread per row) and u (warp per column)
+#pragma unroll
+    for (int q = 0; q < HG_RPT; ++q) {
+      const int i = tid + HC_THREADS * q;
+      if (i >= n) continue;
+      cplx ya = mk(0.0, 0.0), yb = mk(0.0, 0.0);
+      int jl = jl0;
+      for (; jl + 1 < nc; jl += 2) {
+        ya = cfma(colp(jl)[i], v[rank + HC_CS * jl], ya);
+        yb = cfma(colp(jl + 1)[i], v[rank + HC_CS * (jl + 1)], yb);
+      }
+      if (jl < nc) ya = cfma(colp(jl)[i], v[rank + HC_CS * jl], ya);
+      const cplx yi = cadd(ya, yb);
+      for (int r = 0; r < HC_CS; ++r) cluster.map_shared_rank(yp, r)[(par * HC_CS + rank) * HG_MAXN + i] = yi;
+    }
+    for (int jl = jl0 + warp; jl < nc; jl += HC_WARPS) {
+      const cplx* col = colp(jl);
+      cplx p0 = mk(0.0, 0.0), p1 = mk(0.0, 0.0);
+      int r = j0 + lane;
+      for (; r + 32 < n; r += 64) {
+        p0 = cadd(p0, cmulc(v[r], col[r]));
+        p1 = cadd(p1, cmulc(v[r + 32], col[r + 32]));
+      }
+      if (r < n) p0 = cadd(p0, cmulc(v[r], col[r]));
+      const cplx pu = warp_sum_c(cadd(p0, p1));
+      if (lane == 0) us[jl] = pu;
+    }
+    cluster.sync();  // all partial y delivered
+    cplx y[HG_RPT];
+    cplx sl = mk(0.0, 0.0);
+#pragma unroll
+    for (int q = 0; q < HG_RPT; ++q) {
+      const int i = tid + HC_THREADS * q;
+      y[q] = mk(0.0, 0.0);
+      if (i < n) {
+#pragma unroll
+        for (int r = 0; r < HC_CS; ++r) y[q] = cadd(y[q], yp[(par * HC_CS + r) * HG_MAXN + i]);
+        if (i >= j0) sl = cadd(sl, cmulc(vi[q], y[q]));
+      }
+    }
+    const cplx s = block_sum(sl, s_red);
+    const cplx ts = cmul(tau, s), tauc = cconj(tau);
+    for (int jl = jl0 + tid; jl < nc; jl += HC_THREADS) {
+      const cplx vjc = cconj(v[rank + HC_CS * jl]);
+      ca[jl] = cmul(tau, vjc);
+      us[jl] = cmul(tauc, csub(us[jl], cmul(ts, vjc)));
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < HG_RPT; ++q) {
+      const int i = tid + HC_THREADS * q;
+      if (i >= n) continue;
+      const cplx vt = (i >= j0) ? vi[q] : mk(0.0, 0.0);
+#pragma unroll 4
+      for (int jl = jl0; jl < nc; ++jl) {
+        cplx* p = colp(jl) + i;
+        *p = csub(csub(*p, cmul(y[q], ca[jl])), cmul(vt, us[jl]));
+      }
+    }
+    __syncthreads();
+  }
+
+  // --- accumulate Q in place in this CTA's columns of Z
+  __threadfence();
+  cluster.sync();  // every column of H, with its reflector, is in global memory
+  for (int jl = 0; jl < nc; ++jl) {
+    cplx* zc = Z + (size_t)(rank + HC_CS * jl) * n;
+    for (int i = tid; i < n; i += HC_THREADS) zc[i] = mk(i == rank + HC_CS * jl ? 1.0 : 0.0, 0.0);
+  }
+  auto fetch = [&](int k, int i) -> cplx {
+    if (k < 0 || i >= n) return mk(0.0, 0.0);
+    if (i == k + 1) return mk(1.0, 0.0);
+    return i > k + 1 ? H[(size_t)k * n + i] : mk(0.0, 0.0);
+  };
+  cplx vnext[HG_RPT];
+#pragma unroll
+  for (int q = 0; q < HG_RPT; ++q) vnext[q] = fetch(n - 3, tid + HC_THREADS * q);
+  for (int k = n - 3; k >= 0; --k) {
+    const int j0 = k + 1;
+    cplx* v = vb + (k & 1) * HG_MAXN;
+#pragma unroll
+    for (int q = 0; q < HG_RPT; ++q) {
+      const int i = tid + HC_THREADS * q;
+      if (i < n) v[i] = vnext[q];
+      vnext[q] = fetch(k - 1, i);
+    }
+    __syncthreads();
+    const cplx tau = taus[k];
+    if (tau.x == 0.0 && tau.y == 0.0) continue;
+    for (int jl = first_local(j0) + warp; jl < nc; jl += HC_WARPS) {
+      cplx* col = Z + (size_t)(rank + HC_CS * jl) * n;
+      cplx wp = mk(0.0, 0.0);
+      for (int r = j0 + lane; r < n; r += 32) wp = cadd(wp, cmulc(v[r], col[r]));
+      wp = warp_sum_c(wp);
+      const cplx tw = cmul(tau, wp);
+      for (int r = j0 + lane; r < n; r += 32) col[r] = csub(col[r], cmul(v[r], tw));
+    }
+  }
+  __syncthreads();
+  cluster.sync();  // no CTA still reads reflectors from H
+  for (int jl = 0; jl < nc; ++jl) {
+    const int c = rank + HC_CS * jl;
+    cplx* hc = H + (size_t)c * n;
+    for (int i = c + 2 + tid; i < n; i += HC_THREADS) hc[i] = mk(0.0, 0.0);
+  }
+}
+
 }  // namespace
 
-bool hessenberg_cluster_fits(int n) { return n >= 3 && n <= HC_THREADS && hc_layout(n).total <= 227 * 1024; }
+bool hessenberg_cluster_fits(int n) { return n >= 3 && n <= HG_MAXN; }
 
 void hessenberg_cluster_batched(cplx* const* d_H, cplx* const* d_Z, int batch, int n, cudaStream_t st) {
   if (batch <= 0) return;
+  if (n > HC_THREADS || hc_layout(n).total > 227 * 1024) {
+    static bool gconf = false;
+    if (!gconf) {
+      VRC_CUDA_CHECK(cudaFuncSetAttribute(hess_cluster_global_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)HG_SMEM));
+      gconf = true;
+    }
+    for (int b0 = 0; b0 < batch; b0 += 65535) {
+      const int nb = min(65535, batch - b0);
+      hess_cluster_global_kernel<<<dim3(HC_CS, nb), HC_THREADS, HG_SMEM, st>>>(d_H + b0, d_Z + b0, n);
+    }
+    VRC_CUDA_CHECK(cudaGetLastError());
+    return;
+  }
   const size_t smem = hc_layout(n).total;
   static size_t configured = 0;
   if (smem > configured) {
