@@ -891,20 +891,33 @@ void Engine::eig(std::vector<EigReq>& reqs, int n, std::vector<int>* status) {
     for (size_t b = 0; b < B; ++b)
       if (reqs[c0 + b].Q) g.push_back({reqs[c0 + b].Q, W[b], V[b], nullptr, nullptr, ig[b]});
     gemm(g, n, mk(1, 0), mk(0, 0), 0.0);  // V = Q W diag(1/gamma)
+    // W^-1 by inversion; V^-1 = Gamma^-1 W^-1 P (from V = Q W Gamma^-1 and
+    // P Q = W Gamma^2 W^-1: (Gamma^-1 W^-1 P)(Q W Gamma^-1) = I), one GEMM
+    // instead of a second inversion
     std::vector<cplx*> srcs, dsts;
+    std::vector<size_t> inv_req;  // request of each inverted matrix
     for (size_t b = 0; b < B; ++b) {
-      if (reqs[c0 + b].Winv) {
+      const bool wi = reqs[c0 + b].Winv || (reqs[c0 + b].Vinv && reqs[c0 + b].Q);
+      if (wi) {
         srcs.push_back(W[b]);
-        dsts.push_back(reqs[c0 + b].Winv);
-      }
-      if (reqs[c0 + b].Vinv) {
+        dsts.push_back(reqs[c0 + b].Winv ? reqs[c0 + b].Winv : H[b]);  // H is free scratch by now
+        inv_req.push_back(b);
+      } else if (reqs[c0 + b].Vinv) {
         srcs.push_back(V[b]);
         dsts.push_back(reqs[c0 + b].Vinv);
+        inv_req.push_back(b);
       }
     }
     copy(srcs, dsts, n);
     std::vector<int> ist;
     inverse(dsts, n, status ? &ist : nullptr);
+    g.clear();
+    for (size_t q = 0; q < inv_req.size(); ++q) {
+      const size_t b = inv_req[q];
+      if (reqs[c0 + b].Vinv && reqs[c0 + b].Q && srcs[q] == W[b])
+        g.push_back({dsts[q], reqs[c0 + b].P, reqs[c0 + b].Vinv, nullptr, ig[b], nullptr});
+    }
+    gemm(g, n, mk(1, 0), mk(0, 0), 0.0);  // V^-1 = diag(1/gamma) W^-1 P
     for (size_t b = 0; b < B; ++b)
       if (reqs[c0 + b].lam)
         VRC_CUDA_CHECK(cudaMemcpyAsync(reqs[c0 + b].lam, lam[b], (size_t)n * 16, cudaMemcpyDeviceToDevice, stream_));
@@ -915,12 +928,8 @@ void Engine::eig(std::vector<EigReq>& reqs, int n, std::vector<int>* status) {
     if (status) {
       for (size_t b = 0; b < B; ++b)
         if (h[b]) (*status)[c0 + b] = h[b];
-      size_t q = 0;
-      for (size_t b = 0; b < B; ++b) {
-        int nreq = (reqs[c0 + b].Winv ? 1 : 0) + (reqs[c0 + b].Vinv ? 1 : 0);
-        for (int t = 0; t < nreq; ++t, ++q)
-          if (q < ist.size() && ist[q] && !(*status)[c0 + b]) (*status)[c0 + b] = ist[q];
-      }
+      for (size_t q = 0; q < inv_req.size() && q < ist.size(); ++q)
+        if (ist[q] && !(*status)[c0 + inv_req[q]]) (*status)[c0 + inv_req[q]] = ist[q];
     }
   }
 }
