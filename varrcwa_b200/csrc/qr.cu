@@ -396,8 +396,10 @@ __global__ void __launch_bounds__(QR_THREADS, 2)
         for (int idx = tid; idx < nb * nr; idx += QR_THREADS) {
           const int u = idx / nb, b = idx - u * nb;
           const size_t ri = (size_t)s_cur + (size_t)(r0 + u) * nb + b;
-          rot[2 * ri] = s_tau[b * QB + u];
-          rot[2 * ri + 1] = s_v2[b * QB + u];
+          const int kk = m + r0 + u - 3 * b;  // slots of bulges outside the window hold the identity
+          const bool on = kk >= m && kk <= i - 1;
+          rot[2 * ri] = on ? s_tau[b * QB + u] : mk(0.0, 0.0);
+          rot[2 * ri + 1] = on ? s_v2[b * QB + u] : mk(0.0, 0.0);
         }
         // Rest of the active window: columns de+1..i (row transforms) and rows
         // m..ds-1 (column transforms), one bulge chain at a time, leading
@@ -457,7 +459,7 @@ __global__ void __launch_bounds__(QR_THREADS, 2)
 // disjoint pairs and run independently.
 constexpr int RP_THREADS = 128;
 constexpr int RP_NBG = 4;  // bulges per register ring
-constexpr int RP_PFD = 8;  // prefetch depth in rounds
+constexpr int RP_PFD = 7;  // prefetch depth in rounds (ring of PFD + 1 = 8 slots)
 
 __device__ __forceinline__ void cpa16(cplx* smem, const cplx* g) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
@@ -504,8 +506,9 @@ struct ReplayRing {
     }
   }
 
-  template <class Rot>
-  __device__ __forceinline__ void run(int t0, int t1, Rot rot) {
+  // srot: this group's rotations of rounds [t0, t1), NBG (tau, v2) pairs per
+  // round, identity where a bulge is outside the window or beyond the group
+  __device__ __forceinline__ void run(int t0, int t1, const cplx* __restrict__ srot) {
     t1 = min(t1, cnt);
     for (int tb = t0; tb < t1; tb += P) {
 #pragma unroll
@@ -520,16 +523,10 @@ struct ReplayRing {
             if (c >= lo && c <= hi) cpa16(pf + ((t + 1 + PFD) % S) * RP_THREADS, x + (size_t)c * stride);
             cpa_commit();
           }
+          const cplx* rr = srot + 2 * NBG * (t - t0);
 #pragma unroll
-          for (int g = 0; g < NBG; ++g) {
-            cplx tau, v2;
-            rot(t, g, &tau, &v2);
-            const int k = cb - 3 * g;
-            // straight-line code for every bulge: an inactive pair gets the
-            // identity (tau = v2 = 0, entries finite), so the bulges interleave
-            if (!(3 * g <= -rmin && k >= lo && k <= hi - 1)) tau = v2 = mk(0.0, 0.0);
-            rotate2<ROWOP>(w[(tt - 3 * g + 2 * P) % P], w[(tt - 3 * g + 1 + 2 * P) % P], tau, v2);
-          }
+          for (int g = 0; g < NBG; ++g)  // straight-line: inactive pairs carry the identity
+            rotate2<ROWOP>(w[(tt - 3 * g + 2 * P) % P], w[(tt - 3 * g + 1 + 2 * P) % P], rr[2 * g], rr[2 * g + 1]);
           {
             const int q = t - L, c = cb - L;
             if (q >= rmin && c >= lo && c <= hi) x[(size_t)c * stride] = w[(tt - L + 2 * P) % P];
@@ -572,16 +569,15 @@ __device__ __forceinline__ void replay_sweeps(cplx* x, size_t stride, int sel, i
       for (int t0 = 0; t0 < q.R; t0 += RS) {
         const int nr = min(RS, q.R - t0);
         __syncthreads();  // the previous slab is consumed
-        for (int e = threadIdx.x; e < 2 * nr * nb; e += blockDim.x) s_rot[e] = ld(src + 2 * (size_t)t0 * nb + e);
-        __syncthreads();
-        if (active) {
-          auto rf = [&](int t, int g, cplx* tau, cplx* v2) {
-            const int o = 2 * ((t - t0) * nb + min(b0 + g, nb - 1));
-            *tau = s_rot[o];
-            *v2 = s_rot[o + 1];
-          };
-          ring.run(t0, t0 + nr, rf);
+        for (int e = threadIdx.x; e < nr * RP_NBG; e += blockDim.x) {
+          const int u = e / RP_NBG, b = b0 + (e % RP_NBG);
+          const bool on = b < nb;
+          const cplx* q2 = src + 2 * ((size_t)(t0 + u) * nb + b);
+          s_rot[2 * e] = on ? ld(q2) : mk(0.0, 0.0);
+          s_rot[2 * e + 1] = on ? ld(q2 + 1) : mk(0.0, 0.0);
         }
+        __syncthreads();
+        if (active) ring.run(t0, t0 + nr, s_rot);
       }
     }
   }
