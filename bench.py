@@ -40,15 +40,22 @@ def parse():
     p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--batch", type=int, default=128, help="cells per step per GPU")
-    p.add_argument("--workload", default="c2", choices=["c2", "c3"])
-    p.add_argument("--pe", type=float, default=1e-2)
+    p.add_argument("--batch", type=int, default=None,
+                   help="cells per step per GPU (default 128; 8 for c1, whose ~6600 segments per cell are "
+                        "all held until the star reduction)")
+    p.add_argument("--workload", default="c2", choices=["c1", "c2", "c3"])
+    p.add_argument("--pe", type=float, default=None, help="varRCWA tolerance (default 1e-6 for c1, else 1e-2)")
     p.add_argument("--npix", type=int, default=256)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-cells", type=int, default=1, help="cells in the bounded CPU sample")
     p.add_argument("--plain-cells", type=int, default=8,
                    help="cells timed one per call (the plain per-solve form of the metric); 0 skips")
-    return p.parse_args()
+    a = p.parse_args()
+    if a.pe is None:
+        a.pe = 1e-6 if a.workload == "c1" else 1e-2
+    if a.batch is None:
+        a.batch = 8 if a.workload == "c1" else 128
+    return a
 
 
 def make_cells(workload, batch, rank, npix, step_seed=0):
@@ -224,12 +231,15 @@ def metric_name():
 
 
 def workload_config(a, batch):
-    n = 242 if a.workload == "c2" else None
-    return {"workload": ("config-2 pillar cells (11x11 orders, n=242, 256x256 raster)" if a.workload == "c2" else
-                         "config-3 uneven pillar batch (7..15 orders, n=98..450)"),
-            "batch_per_gpu": batch, "n": n, "pe": a.pe, "raster": f"{a.npix}x{a.npix}",
+    names = {"c1": "config-1 2D taper (41 orders, n=82, TE+TM), seeded wavelengths 1.50-1.60 um",
+             "c2": "config-2 pillar cells (11x11 orders, n=242, 256x256 raster)",
+             "c3": "config-3 uneven pillar batch (7..15 orders, n=98..450)"}
+    n = {"c1": 82, "c2": 242}.get(a.workload)
+    return {"workload": names[a.workload], "batch_per_gpu": batch, "n": n, "pe": a.pe,
+            "raster": f"{a.npix}x{a.npix}" if a.workload != "c1" else "2 moving core edges",
             "integrator": "adaptive varRCWA (trisection), Redheffer star products",
-            "output": "per-order R/T, 2 polarisations, incidence from the superstrate",
+            "output": ("the full S-matrix blocks and end bases" if a.workload == "c1" else
+                       "per-order R/T, 2 polarisations, incidence from the superstrate"),
             "l2": "per-step working set (GBs of matrices) exceeds the 126 MB L2; no flush needed"}
 
 
@@ -247,13 +257,20 @@ def run_ours(a, rank, world, local_rank):
     ctx = Context(dev)
     descs = make_cells(a.workload, a.batch, rank, a.npix)
 
+    def solve(cells):
+        # config 1's output is the full S-matrix (its ends are the structure's
+        # own cross-sections, so there are no half-space orders to report)
+        if a.workload == "c1":
+            return ctx.redheffer(cells, pe=a.pe)
+        return ctx.order_powers(cells, method="redheffer", pe=a.pe, side=1)
+
     def barrier():
         if world > 1:
             dist.barrier()
 
     fp64_peak = dgemm_peak_tflops(dev) if rank == 0 else None
     for _ in range(a.warmup):
-        ctx.order_powers(descs, method="redheffer", pe=a.pe, side=1)
+        solve(descs)
     ctx.set_profiling(True)
     clocks = ClockSampler(dev)
     barrier()
@@ -263,7 +280,7 @@ def run_ours(a, rank, world, local_rank):
     launches = 0
     t0 = time.perf_counter()
     for _ in range(a.steps):
-        out = ctx.order_powers(descs, method="redheffer", pe=a.pe, side=1)
+        out = solve(descs)
         t = ctx.timing()
         dev_ms += t["device_ms"]
         launches += t["launches"]
@@ -285,7 +302,10 @@ def run_ours(a, rank, world, local_rank):
     e2e = job_throughput(a.batch, a.steps, world, wall)
     m = 121 if a.workload == "c2" else None
     h2d = sum(len(np.asarray(d.get("eps", [])).tobytes()) for d in descs) + 256 * len(descs)
-    d2h = sum(2 * 2 * d["nx"] * d["ny"] * 8 for d in descs)
+    if a.workload == "c1":  # the S-matrix blocks and both end bases come back
+        d2h = sum(8 * (2 * d["nx"] * d["ny"]) ** 2 * 16 + 2 * 2 * d["nx"] * d["ny"] * 16 for d in descs)
+    else:  # per-order R and T, both polarisations
+        d2h = sum(2 * 2 * d["nx"] * d["ny"] * 8 for d in descs)
     # dominant kernel family and its roofline.  FP64 work on B200 runs either
     # on the DMMA tensor pipe (GEMMs, the inversion's rank-32 updates) or on
     # the FP64 FMA pipe (Hessenberg, QR, back substitution); the two peaks
@@ -332,7 +352,7 @@ def run_ours(a, rank, world, local_rank):
         torch.cuda.synchronize()
         tp = time.perf_counter()
         for d in descs[: a.plain_cells]:
-            ctx.order_powers([d], method="redheffer", pe=a.pe, side=1)
+            solve([d])
         torch.cuda.synchronize()
         tpl = time.perf_counter() - tp
         plain = min(a.plain_cells, len(descs)) / tpl

@@ -52,3 +52,23 @@ def test_full_size_batch_equals_single_calls(ctx):
         p1 = ctx.order_powers([d], method="redheffer", pe=1e-2, side=1)[0]
         for pol in (0, 1):
             assert np.array_equal(b["R"][pol], p1["R"][pol]) and np.array_equal(b["T"][pol], p1["T"][pol])
+
+
+def test_config1_taper_at_its_tolerance(ctx):
+    # config 1 at full size: 41 orders (n = 82), pe = 1e-6, thousands of
+    # segments.  The oracle replay of that tree takes minutes on the CPU, so
+    # the full-size run is checked against the device's plain RCWA with
+    # N = 1000 and 4000 slices: the transmission blocks converge to the
+    # varRCWA result at the slab method's second order.  (Parity with the
+    # oracle on the same structure is tested at pe = 1e-4.)
+    from varrcwa_b200 import structures as st
+    d = st.taper_2d()
+    r = ctx.redheffer([d], pe=1e-6)[0]
+    assert r["status"] == 0 and r["n"] == 82 and r["N"] > 1000
+    F = fourier_blocks(r)
+    err = {}
+    for N in (1000, 4000):
+        G = fourier_blocks(ctx.rcwa([d], N)[0])
+        err[N] = max(relerr(F[k], G[k]) for k in ("Tuu", "Tdd"))
+    assert err[4000] < 1e-5
+    assert err[4000] < err[1000] / 8  # O(1/N^2) convergence onto the varRCWA result

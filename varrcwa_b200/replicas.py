@@ -18,13 +18,17 @@ def cell_seeds(workload: str, batch: int, rank: int, step_seed: int = 0) -> List
     rank so that replicas never solve the same cell."""
     if batch > RANK_STRIDE:
         raise ValueError("batch per rank exceeds the seed stride")
-    base = 1000 * (2 if workload == "c2" else 3) + RANK_STRIDE * rank + step_seed
+    base = 1000 * {"c1": 1, "c2": 2, "c3": 3}[workload] + RANK_STRIDE * rank + step_seed
     return [base + i for i in range(batch)]
 
 
 def make_cells(workload: str, batch: int, rank: int, npix: int, step_seed: int = 0):
+    import numpy as np
+
     from . import structures as st
     seeds = cell_seeds(workload, batch, rank, step_seed)
+    if workload == "c1":  # the config-1 taper at seeded wavelengths around 1.55 um
+        return [st.taper_2d(lam=float(np.random.default_rng(s).uniform(1.50, 1.60))) for s in seeds]
     if workload == "c2":
         return [st.pillar_config2(seed=s, npix=npix) for s in seeds]
     return [st.pillar_config3(seed=s, npix=npix) for s in seeds]
