@@ -282,17 +282,23 @@ void launch_hess(cplx* const* H, cplx* const* Z, int batch, int n, cudaStream_t 
 
 void hessenberg_batched(cplx* const* d_H, cplx* const* d_Z, int batch, int n, cudaStream_t st) {
   if (batch <= 0) return;
-  // Cluster reduction: always for n <= 256 (matrix in shared memory); for
-  // larger n (matrix in L2) when the batch is too small to give every SM two
-  // matrices, or when n is large enough that the single-CTA reduction's
-  // per-matrix latency dominates (measured crossover between 338 and 450).
+  // Cluster or single-CTA reduction, by measured crossovers on B200 (ms per
+  // batch, both variants): the single-CTA kernel wins for n <= 128 at every
+  // batch (4-9x at n = 50..98 once the batch fills the SMs, because eight
+  // CTAs of a few columns each spend the reduction in cluster barriers); for
+  // 128 < n <= 192 and 256 < n < 400 it wins only once the batch gives every
+  // SM two matrices; the cluster kernel wins for 192 < n <= 256 at every batch
+  // (matrix in shared memory) and for n >= 400, where the single-CTA
+  // reduction's per-matrix latency dominates.
   static int sms = 0;
   if (!sms) {
     int dev = 0;
     VRC_CUDA_CHECK(cudaGetDevice(&dev));
     VRC_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   }
-  const bool cluster = hessenberg_cluster_fits(n) && (n <= 256 || n >= 400 || batch < 2 * sms);
+  const bool full = batch >= 2 * sms;
+  const bool cluster = hessenberg_cluster_fits(n) && n > 128 &&
+                       ((n > 192 && n <= 256) || n >= 400 || !full);
   if (cluster && !std::getenv("VRC_HESS_SINGLE_CTA")) {
     hessenberg_cluster_batched(d_H, d_Z, batch, n, st);
     return;
