@@ -183,6 +183,37 @@ int vrc_differential(vrc_context* ctx, int ncells, const vrc_cell* cells, int N,
 int vrc_order_powers(vrc_context* ctx, int ncells, const vrc_cell* cells, int method, double pe, int max_depth,
                      int nslices, int side, int flux_norm, double* R, double* T, int* status);
 
+/* ---- layer stacks: forward solve and adjoint (gradients) -------------------
+ * No counterpart in the reference, which has no gradients; this pair is the C
+ * form of an autograd function.  A stack is nlayers z-uniform layers, each an
+ * npy x npx raster of real permittivity on a uniform (Lx, Ly) grid, between
+ * eps_in (below z0, the incidence side) and eps_out; periodic boundaries.
+ * vrc_stack_forward integrates each stack as the Redheffer chain of its
+ * layers (RedhefferIntegrator.cpp:174-277 on a piecewise-constant structure;
+ * equal to RCWAIntegrator with one slice per layer) and returns per-order
+ * REF / TRN (nstacks * nx*ny each, flux-normalised, order index ny*i + j for
+ * orders (i - (nx-1)/2, j - (ny-1)/2)) for a plane wave (px, py) at normal
+ * incidence from eps_in.  Every stack of a call has the same nx, ny, npx, npy
+ * and nlayers.  What the backward needs stays on the device until the next
+ * vrc_stack_forward on the context.
+ * vrc_stack_backward returns grad_eps (nstacks * nlayers * npy * npx) =
+ * dL/d(eps pixel) for L = sum_k wR[k] REF[k] + wT[k] TRN[k] (wR, wT:
+ * nstacks * nx*ny weights each).  The adjoint covers the star-product chain,
+ * the eigen step (exact first-order layer perturbation in fixed bases, valid
+ * for degenerate eigenvalues) and the Fourier-Toeplitz assembly. */
+typedef struct {
+  double lam, Lx, Ly;
+  int nx, ny;          /* harmonics per axis, odd */
+  int npx, npy;        /* raster of every layer */
+  int nlayers;
+  const double* eps;   /* nlayers * npy * npx, row-major (rows = y), layer 0 at z0 */
+  const double* thick; /* nlayers */
+  vrc_complex eps_in, eps_out;
+} vrc_stack;
+int vrc_stack_forward(vrc_context* ctx, int nstacks, const vrc_stack* stacks, double px, double py, double* REF,
+                      double* TRN, int* status);
+int vrc_stack_backward(vrc_context* ctx, const double* wR, const double* wT, double* grad_eps);
+
 /* ---- instrumentation (no counterpart in the reference) ---------------------
  * Per-kernel-family device time measured with CUDA events on the engine
  * stream, with the algorithmic FP64 flops and bytes of the timed launches. */

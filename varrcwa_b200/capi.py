@@ -23,7 +23,7 @@ EXPORTS = [
     "vrc_create", "vrc_destroy", "vrc_last_error", "vrc_status_string", "vrc_get_timing", "vrc_sample_pq",
     "vrc_wave_solve", "vrc_eig", "vrc_redheffer", "vrc_redheffer_segments", "vrc_get_tree", "vrc_rcwa",
     "vrc_differential", "vrc_order_powers", "vrc_zgemm", "vrc_zinv", "vrc_set_profiling",
-    "vrc_get_kernel_stats", "vrc_eig_noalloc",
+    "vrc_get_kernel_stats", "vrc_eig_noalloc", "vrc_stack_forward", "vrc_stack_backward",
 ]
 
 
@@ -61,6 +61,12 @@ class VrcResult(C.Structure):
     _fields_ = [("Tdd", CP), ("Tuu", CP), ("Rud", CP), ("Rdu", CP), ("W0", CP), ("V0", CP), ("gam0", CP),
                 ("W1", CP), ("V1", CP), ("gam1", CP), ("status", C.c_int), ("n", C.c_int), ("N", C.c_int),
                 ("n_eig", C.c_int), ("n_samples", C.c_int), ("n_nodes", C.c_int)]
+
+
+class VrcStack(C.Structure):
+    _fields_ = [("lam", C.c_double), ("Lx", C.c_double), ("Ly", C.c_double), ("nx", C.c_int), ("ny", C.c_int),
+                ("npx", C.c_int), ("npy", C.c_int), ("nlayers", C.c_int), ("eps", C.POINTER(C.c_double)),
+                ("thick", C.POINTER(C.c_double)), ("eps_in", VrcComplex), ("eps_out", VrcComplex)]
 
 
 class VrcTiming(C.Structure):
@@ -115,6 +121,10 @@ def lib():
     L.vrc_set_profiling.argtypes = [vp, C.c_int]
     L.vrc_get_kernel_stats.argtypes = [vp, C.c_int, C.POINTER(VrcKernelStat)]
     L.vrc_eig_noalloc.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    DP = C.POINTER(C.c_double)
+    L.vrc_stack_forward.argtypes = [vp, C.c_int, C.POINTER(VrcStack), C.c_double, C.c_double, DP, DP,
+                                    C.POINTER(C.c_int)]
+    L.vrc_stack_backward.argtypes = [vp, DP, DP, DP]
     _lib = L
     return L
 
@@ -394,3 +404,37 @@ class Context:
                         "status": int(st[i])})
             off += 2 * m
         return out
+
+    # ---- layer stacks: forward and adjoint ----
+    def stack_forward(self, stacks: List[dict], px: float = 1.0, py: float = 0.0):
+        """Per-order (REF, TRN) of a batch of pixel-layer stacks.  Each stack is a
+        dict with lam, Lx, Ly, nx, ny, layers (list of (npy, npx) real arrays),
+        thick (list), eps_in, eps_out.  Returns (REF, TRN, status) with REF and
+        TRN of shape (nstacks, nx*ny); keeps the state for stack_backward."""
+        keep = []
+        arr = (VrcStack * len(stacks))()
+        for i, d in enumerate(stacks):
+            eps = np.ascontiguousarray(np.stack([np.asarray(a, dtype=np.float64) for a in d["layers"]]))
+            thick = np.ascontiguousarray(np.asarray(d["thick"], dtype=np.float64))
+            keep += [eps, thick]
+            L_, npy, npx = eps.shape
+            arr[i] = VrcStack(float(d["lam"]), float(d["Lx"]), float(d["Ly"]), int(d["nx"]), int(d["ny"]), npx, npy,
+                              L_, _dptr(eps), _dptr(thick), _vc(d.get("eps_in", 1.0)), _vc(d.get("eps_out", 1.0)))
+        m = stacks[0]["nx"] * stacks[0]["ny"]
+        REF = np.zeros((len(stacks), m))
+        TRN = np.zeros((len(stacks), m))
+        st = np.zeros(len(stacks), dtype=np.int32)
+        self._check(self.L.vrc_stack_forward(self.h, len(stacks), arr, float(px), float(py), _dptr(REF), _dptr(TRN),
+                                             st.ctypes.data_as(C.POINTER(C.c_int))))
+        self._stack_shape = (len(stacks), len(stacks[0]["layers"]), *np.asarray(stacks[0]["layers"][0]).shape)
+        return REF, TRN, st
+
+    def stack_backward(self, wR: np.ndarray, wT: np.ndarray):
+        """dL/d(pixel) of L = sum wR*REF + wT*TRN for the last stack_forward;
+        shape (nstacks, nlayers, npy, npx)."""
+        shape = self._stack_shape
+        wR = np.ascontiguousarray(np.broadcast_to(np.asarray(wR, dtype=np.float64), (shape[0], wR.shape[-1])))
+        wT = np.ascontiguousarray(np.broadcast_to(np.asarray(wT, dtype=np.float64), (shape[0], wT.shape[-1])))
+        g = np.zeros(shape)
+        self._check(self.L.vrc_stack_backward(self.h, _dptr(wR), _dptr(wT), _dptr(g)))
+        return g

@@ -435,6 +435,38 @@ int vrc_order_powers(vrc_context* ctx, int ncells, const vrc_cell* cells, int me
   });
 }
 
+int vrc_stack_forward(vrc_context* ctx, int nstacks, const vrc_stack* stacks, double px, double py, double* REF,
+                      double* TRN, int* status) {
+  return guarded(ctx, [&] {
+    if (nstacks < 1 || !stacks || !REF || !TRN) throw vrc::StatusError(VRC_EINVAL, "invalid arguments");
+    std::vector<vrc::Engine::StackSpec> specs(nstacks);
+    for (int c = 0; c < nstacks; ++c) {
+      const vrc_stack& s = stacks[c];
+      if (s.nlayers < 1 || s.npx < 1 || s.npy < 1 || !s.eps || !s.thick)
+        throw vrc::StatusError(VRC_EINVAL, "stack: empty layer list or raster");
+      auto& o = specs[c];
+      o.nx = s.nx; o.ny = s.ny; o.npx = s.npx; o.npy = s.npy; o.L = s.nlayers;
+      o.lambda = s.lam; o.Lx = s.Lx; o.Ly = s.Ly;
+      o.eps.assign(s.eps, s.eps + (size_t)s.nlayers * s.npx * s.npy);
+      o.thick.assign(s.thick, s.thick + s.nlayers);
+      o.eps_in = vrc::mk(s.eps_in.re, s.eps_in.im);
+      o.eps_out = vrc::mk(s.eps_out.re, s.eps_out.im);
+    }
+    Timed tm(ctx);
+    ctx->eng->stack_forward(specs, px, py, REF, TRN, status);
+    tm.done();
+  });
+}
+
+int vrc_stack_backward(vrc_context* ctx, const double* wR, const double* wT, double* grad_eps) {
+  return guarded(ctx, [&] {
+    if (!wR || !wT || !grad_eps) throw vrc::StatusError(VRC_EINVAL, "invalid arguments");
+    Timed tm(ctx);
+    ctx->eng->stack_backward(wR, wT, grad_eps);
+    tm.done();
+  });
+}
+
 int vrc_set_profiling(vrc_context* ctx, int enable) {
   return guarded(ctx, [&] {
     ctx->eng->set_profiling(enable != 0);

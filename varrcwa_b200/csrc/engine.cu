@@ -261,7 +261,7 @@ size_t Engine::batch_budget_bytes() const {
 // ---------------------------------------------------------------------------
 // Batched primitives
 // ---------------------------------------------------------------------------
-void Engine::gemm(std::vector<GemmDesc>& d, int n, cplx alpha, cplx beta, double delta) {
+void Engine::gemm(std::vector<GemmDesc>& d, int n, cplx alpha, cplx beta, double delta, int opA, int opB) {
   if (d.empty()) return;
   const size_t per = 16384;
   for (size_t b0 = 0; b0 < d.size(); b0 += per) {
@@ -269,7 +269,7 @@ void Engine::gemm(std::vector<GemmDesc>& d, int n, cplx alpha, cplx beta, double
     GemmDesc* dd = upload(d.data() + b0, nb);
     const double nn3 = (double)n * n * n;
     Prof pr(*this, "zgemm", 8.0 * nn3 * nb, 48.0 * n * (double)n * nb);
-    zgemm_batched(dd, (int)nb, n, alpha, beta, delta, stream_);
+    zgemm_batched(dd, (int)nb, n, alpha, beta, delta, stream_, -1, opA, opB);
   }
 }
 
@@ -688,6 +688,15 @@ void Engine::assemble(std::vector<SampleReq>& reqs, std::vector<int>* status) {
       // fe33^{-1} (BDCSVD solve of the square system, Layer.cpp:84-86)
       std::vector<int> inv_status;
       inverse(fe33, m, status ? &inv_status : nullptr);
+      {
+        std::vector<cplx*> ks, kd;
+        for (size_t b = 0; b < B; ++b)
+          if (reqs[idx[c0 + b]].keep_fe33inv) {
+            ks.push_back(fe33[b]);
+            kd.push_back(reqs[idx[c0 + b]].keep_fe33inv);
+          }
+        copy(ks, kd, m);
+      }
       std::vector<cplx*> Pp(B), Qp(B);
       for (size_t b = 0; b < B; ++b) {
         Pp[b] = reqs[idx[c0 + b]].P;

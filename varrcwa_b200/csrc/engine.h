@@ -114,7 +114,8 @@ class Engine {
   size_t batch_budget_bytes() const;
 
   // batched primitives
-  void gemm(std::vector<GemmDesc>& d, int n, cplx alpha, cplx beta, double delta);
+  // opA / opB = 1: that operand enters as its conjugate transpose.
+  void gemm(std::vector<GemmDesc>& d, int n, cplx alpha, cplx beta, double delta, int opA = 0, int opB = 0);
   void inverse(const std::vector<cplx*>& mats, int n, std::vector<int>* status);
   void copy(const std::vector<cplx*>& src, const std::vector<cplx*>& dst, int n);
   void axpby(const std::vector<const cplx*>& A, const std::vector<const cplx*>& B, const std::vector<cplx*>& C,
@@ -144,6 +145,7 @@ class Engine {
     cplx eps_h;
     cplx* P;
     cplx* Q;
+    cplx* keep_fe33inv = nullptr;  // optional copy of fe33^-1 (m x m; periodic cells)
   };
   void assemble(std::vector<SampleReq>& reqs, std::vector<int>* status);
 
@@ -235,6 +237,26 @@ class Engine {
   void order_powers(const std::vector<CellSpec>& cells, const std::vector<CellResult>& res, int side,
                     int flux_norm, std::vector<std::vector<double>>& R, std::vector<std::vector<double>>& T);
 
+  // ---- layer stacks of z-uniform pixel rasters: forward and adjoint ----
+  // Layer l (0 nearest z0) holds an npy x npx raster of real permittivity on a
+  // uniform (Lx, Ly) grid and has thickness thick[l]; eps_in below z0 (the
+  // incidence side), eps_out above.  Periodic boundaries.
+  struct StackSpec {
+    int nx = 1, ny = 1, npx = 1, npy = 1, L = 0;
+    double lambda = 1.0, Lx = 1.0, Ly = 1.0;
+    std::vector<double> eps;    // L * npy * npx, row-major per layer (rows = y)
+    std::vector<double> thick;  // L
+    cplx eps_in{1.0, 0.0}, eps_out{1.0, 0.0};
+  };
+  // Per-order (REF, TRN) of every stack (m each) for incidence (px, py) from
+  // eps_in; keeps what stack_backward needs until the next stack_forward.
+  void stack_forward(const std::vector<StackSpec>& stacks, double px, double py, double* REF, double* TRN,
+                     int* status);
+  // Gradient of L = sum_k wR[k] REF[k] + wT[k] TRN[k] (m weights each per
+  // stack) with respect to every pixel of every layer (L * npy * npx per stack).
+  void stack_backward(const double* wR, const double* wT, double* grad);
+  void release_stack_tape();
+
   // counters
   long long launches = 0;
 
@@ -298,6 +320,28 @@ class Engine {
   struct EndBasis {
     cplx *W, *V, *Winv, *Vinv, *gam;
   };
+  // Device state of the last stack_forward (one block per stack).
+  struct StackLayer {
+    cplx *P, *Q, *W, *V, *Winv, *Vinv, *gam, *A, *B, *Ainv, *x, *fe33inv, *eps;
+    cplx* seg[4];  // projected layer blocks (tdd, tuu, rud, rdu)
+    cplx* pre[4];  // chain before this layer's star product
+  };
+  struct StackCell {
+    char* mem = nullptr;
+    size_t bytes = 0;
+    EndBasis e0, e1;
+    std::vector<StackLayer> lay;
+    cplx *Sc[4], *S[4], *Ar, *Br, *Mrinv;
+    double *alpha, *beta;
+  };
+  struct StackTape {
+    int C = 0, L = 0, n = 0, m = 0, nx = 0, ny = 0, npx = 0, npy = 0;
+    double px = 1.0, py = 0.0;
+    std::vector<StackSpec> specs;
+    std::vector<StackCell> cells;
+    std::vector<int> status;
+  };
+  StackTape tape_;
 };
 
 template <class T>

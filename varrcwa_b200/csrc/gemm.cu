@@ -5,7 +5,8 @@
 // for column-major n x n operands (every contraction of the hot path is
 // square: projections, star products, perturbation terms, P*Q), or with an
 // inner dimension kdim != n (A is n x kdim, B is kdim x n) for the rank-kdim
-// updates of the blocked inversion.  One CTA
+// updates of the blocked inversion.  Either operand may be taken as its
+// conjugate transpose (square operands only; used by the adjoint).  One CTA
 // computes a 64 x 64 complex tile; operands are staged through shared memory
 // by 16-byte cp.async copies in a 3-stage pipeline.  The complex product
 // uses three real products (P1 = Ar Br, P2 = Ai Bi, P3 = (Ar+Ai)(Br+Bi);
@@ -44,6 +45,10 @@ __device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, doubl
       : "d"(a0), "d"(a1), "d"(b0));
 }
 
+// OPA / OPB: 0 = the operand as stored, 1 = its conjugate transpose.  A
+// transposed operand is staged with consecutive threads along its stored
+// columns (coalesced) and conjugated when fragments are read.
+template <int OPA, int OPB>
 __global__ void __launch_bounds__(NTHREADS, 2)
     zgemm_kernel(const GemmDesc* __restrict__ descs, int n, int kdim, cplx alpha, cplx beta, double delta) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -70,16 +75,32 @@ __global__ void __launch_bounds__(NTHREADS, 2)
 #pragma unroll
     for (int i = 0; i < 2; ++i) {
       int idx = tid + i * NTHREADS;
-      // A tile: 64 rows x 8 cols, consecutive threads -> consecutive rows.
-      int r = idx & 63, k = idx >> 6;
-      int gr = m0 + r, gk = k0 + k;
-      bool va = (gr < n) && (gk < kdim);
-      cp_async16(as + k * LDA + r, va ? (const void*)(A + (size_t)gk * n + gr) : (const void*)A, va);
-      // B tile: 8 rows x 64 cols, consecutive threads -> consecutive k.
-      int kb = idx & 7, c = idx >> 3;
-      int gkb = k0 + kb, gc = n0 + c;
-      bool vb = (gkb < kdim) && (gc < n);
-      cp_async16(bs + kb * LDB + c, vb ? (const void*)(B + (size_t)gc * kdim + gkb) : (const void*)B, vb);
+      if (OPA == 0) {
+        // A tile: 64 rows x 8 cols, consecutive threads -> consecutive rows.
+        int r = idx & 63, k = idx >> 6;
+        int gr = m0 + r, gk = k0 + k;
+        bool va = (gr < n) && (gk < kdim);
+        cp_async16(as + k * LDA + r, va ? (const void*)(A + (size_t)gk * n + gr) : (const void*)A, va);
+      } else {
+        // op(A)(r, k) = conj(A(k, r)), stored at A[r * n + k]: threads along k.
+        int k = idx & 7, r = idx >> 3;
+        int gr = m0 + r, gk = k0 + k;
+        bool va = (gr < n) && (gk < kdim);
+        cp_async16(as + k * LDA + r, va ? (const void*)(A + (size_t)gr * n + gk) : (const void*)A, va);
+      }
+      if (OPB == 0) {
+        // B tile: 8 rows x 64 cols, consecutive threads -> consecutive k.
+        int kb = idx & 7, c = idx >> 3;
+        int gkb = k0 + kb, gc = n0 + c;
+        bool vb = (gkb < kdim) && (gc < n);
+        cp_async16(bs + kb * LDB + c, vb ? (const void*)(B + (size_t)gc * kdim + gkb) : (const void*)B, vb);
+      } else {
+        // op(B)(k, c) = conj(B(c, k)), stored at B[k * n + c]: threads along c.
+        int c = idx & 63, kb = idx >> 6;
+        int gkb = k0 + kb, gc = n0 + c;
+        bool vb = (gkb < kdim) && (gc < n);
+        cp_async16(bs + kb * LDB + c, vb ? (const void*)(B + (size_t)gkb * n + gc) : (const void*)B, vb);
+      }
     }
   };
 
@@ -114,9 +135,16 @@ __global__ void __launch_bounds__(NTHREADS, 2)
         int row = wm * 32 + mt * 16 + g;
         af[mt][0] = as[(ks + tig) * LDA + row];
         af[mt][1] = as[(ks + tig) * LDA + row + 8];
+        if (OPA) {
+          af[mt][0].y = -af[mt][0].y;
+          af[mt][1].y = -af[mt][1].y;
+        }
       }
 #pragma unroll
-      for (int nt = 0; nt < 2; ++nt) bf[nt] = bs[(ks + tig) * LDB + wn * 16 + nt * 8 + g];
+      for (int nt = 0; nt < 2; ++nt) {
+        bf[nt] = bs[(ks + tig) * LDB + wn * 16 + nt * 8 + g];
+        if (OPB) bf[nt].y = -bf[nt].y;
+      }
 #pragma unroll
       for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
@@ -155,20 +183,28 @@ __global__ void __launch_bounds__(NTHREADS, 2)
 }  // namespace
 
 void zgemm_batched(const GemmDesc* d_descs, int batch, int n, cplx alpha, cplx beta, double delta,
-                   cudaStream_t stream, int kdim) {
+                   cudaStream_t stream, int kdim, int opA, int opB) {
   if (kdim < 0) kdim = n;
+  if ((opA || opB) && kdim != n) throw StatusError(ST_EINVAL, "transposed GEMM operands must be square");
   static bool configured = false;
   if (!configured) {
-    VRC_CUDA_CHECK(cudaFuncSetAttribute(zgemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    VRC_CUDA_CHECK(cudaFuncSetAttribute(zgemm_kernel<0, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        SMEM_BYTES));
+    VRC_CUDA_CHECK(cudaFuncSetAttribute(zgemm_kernel<1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        SMEM_BYTES));
+    VRC_CUDA_CHECK(cudaFuncSetAttribute(zgemm_kernel<0, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        SMEM_BYTES));
+    VRC_CUDA_CHECK(cudaFuncSetAttribute(zgemm_kernel<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         SMEM_BYTES));
     configured = true;
   }
   if (batch <= 0) return;
+  auto kern = opA ? (opB ? zgemm_kernel<1, 1> : zgemm_kernel<1, 0>) : (opB ? zgemm_kernel<0, 1> : zgemm_kernel<0, 0>);
   int tiles = ((n + BM - 1) / BM) * ((n + BN - 1) / BN);
   for (int b0 = 0; b0 < batch; b0 += 65535) {
     int nb = batch - b0 < 65535 ? batch - b0 : 65535;
     dim3 grid(tiles, nb);
-    zgemm_kernel<<<grid, NTHREADS, SMEM_BYTES, stream>>>(d_descs + b0, n, kdim, alpha, beta, delta);
+    kern<<<grid, NTHREADS, SMEM_BYTES, stream>>>(d_descs + b0, n, kdim, alpha, beta, delta);
   }
   VRC_CUDA_CHECK(cudaGetLastError());
 }

@@ -15,8 +15,9 @@ struct GemmDesc {
   const cplx* rs;   // optional row scale (n)
   const cplx* cs;   // optional column scale (n)
 };
+// opA / opB = 1 takes that operand as its conjugate transpose (kdim == n).
 void zgemm_batched(const GemmDesc* d_descs, int batch, int n, cplx alpha, cplx beta, double delta,
-                   cudaStream_t stream, int kdim = -1);  // kdim < 0: n
+                   cudaStream_t stream, int kdim = -1, int opA = 0, int opB = 0);  // kdim < 0: n
 
 // ---- inverse (in place) -------------------------------------------------------
 int zinv_panel_width(int n);
@@ -109,5 +110,45 @@ void axpby_batched(const cplx* const* A, const cplx* const* B, cplx* const* C, c
                    int batch, int n, cudaStream_t st);
 void order_power_batched(const PowerDesc* d, int batch, int m, cudaStream_t st);
 void matvec_batched(const MatVecDesc* d, int batch, int n, cudaStream_t st);
+
+// ---- layer-stack forward / adjoint (adjoint.cu) ------------------------------------
+// out = diag(rs) A diag(cs); rs / cs (or an entry of them) may be null.
+void scale_batched(const cplx* const* A, const cplx* const* rs, const cplx* const* cs, cplx* const* out, int batch,
+                   int n, cudaStream_t st);
+// out_i = exp(i gam_i t)
+void phase_vec_batched(const cplx* const* gam, const double* t, cplx* const* out, int batch, int n, cudaStream_t st);
+struct LayerAdjDesc {
+  const cplx *gtdd, *gtuu, *grud, *grdu;  // own-basis block adjoints
+  const cplx* gam;
+  cplx *gS, *gD;  // gA + gB, gA - gB
+  double d, k0;
+};
+void layer_adjoint_batched(const LayerAdjDesc* d, int batch, int n, cudaStream_t st);
+struct PQAdjDesc {
+  const cplx *gP, *gQ;
+  const double *alpha, *beta;
+  cplx *g11, *g22, *Z;  // m x m each
+  double k0;
+};
+void pq_adjoint_batched(const PQAdjDesc* d, int batch, int m, cudaStream_t st);
+struct PixAdjDesc {
+  const cplx* eps;                 // npy x npx, row-major (rows = y strips)
+  const cplx *g11, *g22, *g33;     // m x m
+  double* grad;                    // npy x npx
+  double Lx, Ly;
+};
+bool pixel_adjoint_fits(int nx, int ny, int npx, int npy);
+void pixel_adjoint_batched(const PixAdjDesc* d, int batch, int nx, int ny, int npx, int npy, cudaStream_t st);
+struct StackPowerDesc {
+  const cplx *W0, *W0inv, *W1, *Tuu, *Rdu;
+  const double *alpha, *beta;
+  const double *wR, *wT;  // adjoint weights (m), used when adj
+  double *REF, *TRN;      // m
+  cplx *gRdu, *gTuu;      // n x n, written when adj
+  cplx eps_in, eps_out;
+  double k0, px, py;
+  int nx, ny;
+};
+void stack_power_batched(const StackPowerDesc* d, int batch, int m, int adj, cudaStream_t st);
 
 }  // namespace vrc
