@@ -15,6 +15,12 @@ wall time of the same C-ABI calls from host structure descriptors to host
 order powers.  Multi-GPU runs are independent replicas (one process per
 GPU, disjoint cell seeds, no collective on the data path).
 
+`--workload c4` measures the other half of the metric: forward + adjoint
+solves of config-4 freeform metagratings (600 nm period, 633 nm, 9x9 orders,
+four 150 nm layers of 64x64 permittivity pixels) -- per-order powers and the
+gradient of T(+1,0) with respect to all 16384 pixels per stack.  The default
+config-2 line carries a short run of it under "fwd_adjoint".
+
 `--impl reference` times the CPU restatement of the reference algorithm
 (the oracle) on this machine's host cores on the same workload.
 """
@@ -43,13 +49,14 @@ def parse():
     p.add_argument("--batch", type=int, default=None,
                    help="cells per step per GPU (default 128; 8 for c1, whose ~6600 segments per cell are "
                         "all held until the star reduction)")
-    p.add_argument("--workload", default="c2", choices=["c1", "c2", "c3"])
+    p.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4"])
     p.add_argument("--pe", type=float, default=None, help="varRCWA tolerance (default 1e-6 for c1, else 1e-2)")
     p.add_argument("--npix", type=int, default=256)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-cells", type=int, default=1, help="cells in the bounded CPU sample")
     p.add_argument("--plain-cells", type=int, default=8,
                    help="cells timed one per call (the plain per-solve form of the metric); 0 skips")
+    p.add_argument("--no-adjoint", action="store_true", help="skip the fwd_adjoint sub-measurement of the c2 line")
     a = p.parse_args()
     if a.pe is None:
         a.pe = 1e-6 if a.workload == "c1" else 1e-2
@@ -164,11 +171,28 @@ def _oracle_cell(args):
     return float(R.sum() + T.sum())
 
 
+def _oracle_stack(desc):
+    """Forward + adjoint of one config-4 stack through the oracle."""
+    import numpy as np
+    from oracle.stack_adjoint import Stack, order_index, stack_backward, stack_forward
+    st = Stack(desc["lam"], desc["nx"], desc["ny"], desc["Lx"], desc["Ly"], desc["layers"], desc["thick"],
+               desc["eps_in"], desc["eps_out"])
+    R, T, tp = stack_forward(st)
+    m = desc["nx"] * desc["ny"]
+    wT = np.zeros(m)
+    wT[order_index(desc["nx"], desc["ny"], 1, 0)] = 1.0
+    g = stack_backward(st, tp, np.zeros(m), wT)
+    return float(T.sum() + sum(float(x.sum()) for x in g))
+
+
 def cpu_sample(descs, pe):
     """Time the oracle on the given cells with all host threads (BLAS)."""
     t0 = time.perf_counter()
     for d in descs:
-        _oracle_cell((d, pe))
+        if "layers" in d:
+            _oracle_stack(d)
+        else:
+            _oracle_cell((d, pe))
     return time.perf_counter() - t0
 
 
@@ -184,22 +208,30 @@ def run_reference(a, rank, world):
     os.environ["MKL_NUM_THREADS"] = "1"
     ctxm = mp.get_context("spawn")
     with ctxm.Pool(workers) as pool:
-        # warm-up: one small task per worker (imports, first BLAS call)
-        for _ in range(a.warmup):
-            pool.map(_oracle_cell, [(d, 0.5) for d in make_cells(a.workload, workers, rank, 16)])
-        t0 = time.perf_counter()
-        for _ in range(a.steps):
-            pool.map(_oracle_cell, [(d, a.pe) for d in descs])
-        dt = time.perf_counter() - t0
+        if a.workload == "c4":
+            pool.map(_oracle_stack, descs[:workers])  # warm-up: imports, first BLAS call
+            t0 = time.perf_counter()
+            for _ in range(a.steps):
+                pool.map(_oracle_stack, descs)
+            dt = time.perf_counter() - t0
+        else:
+            # warm-up: one small task per worker (imports, first BLAS call)
+            for _ in range(a.warmup):
+                pool.map(_oracle_cell, [(d, 0.5) for d in make_cells(a.workload, workers, rank, 16)])
+            t0 = time.perf_counter()
+            for _ in range(a.steps):
+                pool.map(_oracle_cell, [(d, a.pe) for d in descs])
+            dt = time.perf_counter() - t0
     value = a.steps * len(descs) / dt
     line = {
-        "impl": "reference", "metric": metric_name(), "value": value, "unit": "solves/s", "n_gpus": a.gpus,
+        "impl": "reference", "metric": metric_name(a.workload), "value": value, "unit": unit_name(a.workload),
+        "n_gpus": a.gpus,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * dt / a.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "complex128", "data": "synthetic",
         "config": workload_config(a, len(descs)),
-        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": workers, "kind": "port",
+        "cpu_baseline": {"value": value, "unit": unit_name(a.workload), "cores": workers, "kind": "port",
                          "sample": f"{len(descs)} cells per step, one per process (spawn), single-threaded BLAS"},
-        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "e2e": {"value": value, "unit": unit_name(a.workload), "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
@@ -226,11 +258,23 @@ def profiled_traffic(family, flops_per_launch):
     return kv["bytes_per_matrix"] * flops_per_launch / kv["flops_per_matrix"]
 
 
-def metric_name():
+def metric_name(workload="c2"):
+    if workload == "c4":
+        return "batched fwd+adjoint grads/s (FP64 stack solve, per-order T/R and d T(+1,0) / d pixel)"
     return "batched S-matrix solves/s (FP64 varRCWA forward, per-order T/R)"
 
 
+def unit_name(workload="c2"):
+    return "grads/s" if workload == "c4" else "solves/s"
+
+
 def workload_config(a, batch):
+    if a.workload == "c4":
+        return {"workload": "config-4 freeform metagrating stacks (9x9 orders, n=162, 4 layers x 64x64 pixels, "
+                            "600 nm period, 633 nm, air -> SiO2)", "batch_per_gpu": batch, "n": 162,
+                "integrator": "Redheffer chain of z-uniform layers (one eigen-solve per layer), star products",
+                "output": "per-order R/T (x-polarised incidence) and dT(+1,0)/d(eps) for all 16384 pixels",
+                "l2": "per-step working set (GBs of matrices) exceeds the 126 MB L2; no flush needed"}
     names = {"c1": "config-1 2D taper (41 orders, n=82, TE+TM), seeded wavelengths 1.50-1.60 um",
              "c2": "config-2 pillar cells (11x11 orders, n=242, 256x256 raster)",
              "c3": "config-3 uneven pillar batch (7..15 orders, n=98..450)"}
@@ -257,12 +301,7 @@ def run_ours(a, rank, world, local_rank):
     ctx = Context(dev)
     descs = make_cells(a.workload, a.batch, rank, a.npix)
 
-    def solve(cells):
-        # config 1's output is the full S-matrix (its ends are the structure's
-        # own cross-sections, so there are no half-space orders to report)
-        if a.workload == "c1":
-            return ctx.redheffer(cells, pe=a.pe)
-        return ctx.order_powers(cells, method="redheffer", pe=a.pe, side=1)
+    solve = make_solver(ctx, a.workload, a.pe, a.batch)
 
     def barrier():
         if world > 1:
@@ -271,6 +310,9 @@ def run_ours(a, rank, world, local_rank):
     fp64_peak = dgemm_peak_tflops(dev) if rank == 0 else None
     for _ in range(a.warmup):
         solve(descs)
+    adjoint = None
+    if a.workload == "c2" and world == 1 and not a.no_adjoint:
+        adjoint = measure_fwd_adjoint(ctx, rank, a.no_cpu_baseline)
     ctx.set_profiling(True)
     clocks = ClockSampler(dev)
     barrier()
@@ -280,10 +322,9 @@ def run_ours(a, rank, world, local_rank):
     launches = 0
     t0 = time.perf_counter()
     for _ in range(a.steps):
-        out = solve(descs)
-        t = ctx.timing()
-        dev_ms += t["device_ms"]
-        launches += t["launches"]
+        out, ms, nl = solve(descs)
+        dev_ms += ms
+        launches += nl
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     barrier()
@@ -304,6 +345,10 @@ def run_ours(a, rank, world, local_rank):
     h2d = sum(len(np.asarray(d.get("eps", [])).tobytes()) for d in descs) + 256 * len(descs)
     if a.workload == "c1":  # the S-matrix blocks and both end bases come back
         d2h = sum(8 * (2 * d["nx"] * d["ny"]) ** 2 * 16 + 2 * 2 * d["nx"] * d["ny"] * 16 for d in descs)
+    elif a.workload == "c4":  # R, T of one polarisation and the pixel gradient; weights go up
+        h2d = sum(sum(np.asarray(x).nbytes for x in d["layers"]) + 8 * len(d["thick"]) + 2 * 8 * d["nx"] * d["ny"]
+                  for d in descs)
+        d2h = sum(2 * 8 * d["nx"] * d["ny"] + sum(np.asarray(x).nbytes for x in d["layers"]) for d in descs)
     else:  # per-order R and T, both polarisations
         d2h = sum(2 * 2 * d["nx"] * d["ny"] * 8 for d in descs)
     # dominant kernel family and its roofline.  FP64 work on B200 runs either
@@ -334,12 +379,13 @@ def run_ours(a, rank, world, local_rank):
                      "launches": v["launches"],
                      "tflops": round(v["flops"] / (v["ms"] * 1e-3) / 1e12, 3) if v["flops"] and v["ms"] else None}
                  for k, v in sorted(stats.items(), key=lambda kv: -kv[1]["ms"])}
+    unit = unit_name(a.workload)
     line = {
-        "metric": metric_name(), "value": value, "unit": "solves/s", "n_gpus": world, "steps": a.steps,
+        "metric": metric_name(a.workload), "value": value, "unit": unit, "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": dev_ms / a.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "complex128", "data": "synthetic",
         "config": workload_config(a, a.batch), "parallelism": f"replicas x{world}",
-        "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "e2e": {"value": e2e, "unit": unit, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches, "roofline": roof, "clocks": clk, "kernel_breakdown": breakdown,
         "statuses_nonzero": int(sum(1 for s in statuses if s)),
     }
@@ -356,17 +402,88 @@ def run_ours(a, rank, world, local_rank):
         torch.cuda.synchronize()
         tpl = time.perf_counter() - tp
         plain = min(a.plain_cells, len(descs)) / tpl
-        line["plain_per_solve"] = {"value": plain, "unit": "solves/s", "cells": min(a.plain_cells, len(descs)),
+        line["plain_per_solve"] = {"value": plain, "unit": unit, "cells": min(a.plain_cells, len(descs)),
                                    "form": "one cell per C-ABI call, same GPU, host buffers"}
         line["batched_over_plain"] = e2e / plain
     if world == 1 and not a.no_cpu_baseline:
         sample = descs[: a.cpu_cells]
         dt = cpu_sample(sample, a.pe)
-        line["cpu_baseline"] = {"value": len(sample) / dt, "unit": "solves/s", "cores": os.cpu_count(),
+        line["cpu_baseline"] = {"value": len(sample) / dt, "unit": unit, "cores": os.cpu_count(),
                                 "kind": "port",
                                 "sample": f"{len(sample)} cell(s) of the same workload through the numpy oracle "
                                           f"(OpenBLAS threads = host cores), {dt:.1f} s"}
+    if adjoint is not None:
+        line["fwd_adjoint"] = adjoint
     print(json.dumps(line), flush=True)
+
+
+def make_solver(ctx, workload, pe, batch):
+    """One step of the workload through the C ABI: returns (per-cell results,
+    device ms, kernel launches) of the call(s)."""
+    import numpy as np
+    if workload == "c4":
+        nx = ny = 9
+        k = ny * (1 + (nx - 1) // 2) + (ny - 1) // 2  # order (+1, 0)
+        wT = np.zeros((batch, nx * ny))
+        wT[:, k] = 1.0
+        wR = np.zeros((batch, nx * ny))
+
+        def solve(cells):
+            _, _, st = ctx.stack_forward(cells)
+            t1 = ctx.timing()
+            ctx.stack_backward(wR[: len(cells)], wT[: len(cells)])
+            t2 = ctx.timing()
+            return ([{"status": int(x)} for x in st], t1["device_ms"] + t2["device_ms"],
+                    t1["launches"] + t2["launches"])
+        return solve
+
+    def solve(cells):
+        # config 1's output is the full S-matrix (its ends are the structure's
+        # own cross-sections, so there are no half-space orders to report)
+        if workload == "c1":
+            out = ctx.redheffer(cells, pe=pe)
+        else:
+            out = ctx.order_powers(cells, method="redheffer", pe=pe, side=1)
+        t = ctx.timing()
+        return out, t["device_ms"], t["launches"]
+    return solve
+
+
+def measure_fwd_adjoint(ctx, rank, no_cpu, batch=128, steps=3, warmup=3, plain=4):
+    """Short config-4 forward+adjoint measurement for the default line."""
+    import torch
+    cells = make_cells("c4", batch, rank, 64)
+    solve = make_solver(ctx, "c4", None, batch)
+    for _ in range(warmup):
+        solve(cells)
+    torch.cuda.synchronize()
+    dev_ms = 0.0
+    launches = 0
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        _, ms, nl = solve(cells)
+        dev_ms += ms
+        launches += nl
+    wall = time.perf_counter() - t0
+    tp = time.perf_counter()
+    for d in cells[:plain]:
+        solve([d])
+    tpl = time.perf_counter() - tp
+    out = {"metric": metric_name("c4"), "value": batch * steps / (dev_ms * 1e-3), "unit": "grads/s",
+           "e2e": {"value": batch * steps / wall, "unit": "grads/s"}, "steps": steps, "warmup": warmup,
+           "ms_per_step": dev_ms / steps, "gpu_launches": launches,
+           "config": {"workload": "config-4 freeform metagrating stacks (9x9 orders, n=162, 4 layers x 64x64 "
+                                  "pixels)", "batch_per_gpu": batch,
+                      "output": "per-order R/T and dT(+1,0)/d(eps) for all 16384 pixels"},
+           "plain_per_solve": {"value": plain / tpl, "unit": "grads/s", "cells": plain,
+                               "form": "one stack per forward+backward C-ABI pair"},
+           "batched_over_plain": (batch * steps / wall) / (plain / tpl)}
+    if not no_cpu:
+        dt = cpu_sample(cells[:1], None)
+        out["cpu_baseline"] = {"value": 1.0 / dt, "unit": "grads/s", "cores": os.cpu_count(), "kind": "port",
+                               "sample": f"1 stack, oracle forward + adjoint (OpenBLAS threads = host cores), "
+                                         f"{dt:.2f} s; central differences would need 2 x 16384 solves"}
+    return out
 
 
 def main():

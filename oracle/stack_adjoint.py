@@ -407,17 +407,3 @@ def stack_backward(st: Stack, tp: Tape, wR, wT, want_pq=False):
 def order_index(nx, ny, ox, oy):
     """Index of diffraction order (ox, oy) in the per-order power vectors."""
     return ny * (ox + (nx - 1) // 2) + (oy + (ny - 1) // 2)
-
-
-def smooth_pixels(seed, npx, npy, sigma=3.0, beta=8.0, lo=2.085, hi=12.11):
-    """Freeform layer permittivity: seeded uniform noise, periodic Gaussian
-    smoothing (sigma in pixels), sigmoid threshold (beta), mapped to [lo, hi]."""
-    rng = np.random.default_rng(seed)
-    u = rng.uniform(0.0, 1.0, (npy, npx))
-    ky = np.fft.fftfreq(npy)[:, None]
-    kx = np.fft.fftfreq(npx)[None, :]
-    g = np.exp(-2.0 * (PI * sigma) ** 2 * (kx * kx + ky * ky))
-    s = np.fft.ifft2(np.fft.fft2(u) * g).real
-    s = (s - s.mean()) / (s.std() + 1e-30)
-    t = 1.0 / (1.0 + np.exp(-beta * s))
-    return lo + (hi - lo) * t

@@ -5,7 +5,8 @@ perturbed stacks."""
 import numpy as np
 import pytest
 
-from oracle.stack_adjoint import Stack, order_index, smooth_pixels, stack_backward, stack_forward
+from oracle.stack_adjoint import Stack, order_index, stack_backward, stack_forward
+from varrcwa_b200.structures import smooth_pixels
 
 pytestmark = pytest.mark.gpu
 

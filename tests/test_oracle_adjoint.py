@@ -4,7 +4,8 @@ oracle's RCWA integrator, the adjoint against central finite differences
 import numpy as np
 import pytest
 
-from oracle.stack_adjoint import Stack, order_index, smooth_pixels, stack_backward, stack_forward
+from oracle.stack_adjoint import Stack, order_index, stack_backward, stack_forward
+from varrcwa_b200.structures import smooth_pixels
 from oracle.varrcwa_oracle import homogeneous_basis, order_powers, rcwa_compute
 
 LAM, PER = 0.633, 0.6

@@ -153,3 +153,30 @@ def waveguide_pml(seed, norders=21, ncontrol=64, length=20.0, cell=(4.0, 2.0),
     return dict(kind="grid", lam=lam, nx=norders, ny=norders, pml=True, x=x, y=y, eps=eps,
                 xrules=[(2, zs, cx - 0.5 * widths), (3, zs, cx + 0.5 * widths)],
                 z0=0.0, z1=length, end0=None, end1=None, widths=widths)
+
+
+def smooth_pixels(seed, npx, npy, sigma=3.0, beta=8.0, lo=2.085, hi=12.11):
+    """Freeform layer permittivity: seeded uniform noise, periodic Gaussian
+    smoothing (sigma in pixels), sigmoid threshold (beta) of the standardised
+    field, mapped to [lo, hi].  Returns an (npy, npx) real array."""
+    rng = np.random.default_rng(seed)
+    u = rng.uniform(0.0, 1.0, (npy, npx))
+    ky = np.fft.fftfreq(npy)[:, None]
+    kx = np.fft.fftfreq(npx)[None, :]
+    g = np.exp(-2.0 * (math.pi * sigma) ** 2 * (kx * kx + ky * ky))
+    f = np.fft.ifft2(np.fft.fft2(u) * g).real
+    f = (f - f.mean()) / (f.std() + 1e-30)
+    t = 1.0 / (1.0 + np.exp(-beta * f))
+    return lo + (hi - lo) * t
+
+
+def metagrating_c4(seed=4000, npix=64, nlayers=4):
+    """Freeform metagrating of config 4: 600 nm square period, 633 nm, 9x9
+    orders (n = 162), four 150 nm layers of npix x npix pixels (smoothed
+    thresholded noise in [2.085, 12.11], layer l seeded by (seed, l)).
+    Incidence from air below; transmission into the SiO2 substrate (eps
+    2.085), where the (+1, 0) order propagates (it is evanescent in air at
+    this period)."""
+    layers = [smooth_pixels([seed, l], npix, npix) for l in range(nlayers)]
+    return dict(lam=0.633, Lx=0.6, Ly=0.6, nx=9, ny=9, layers=layers, thick=[0.15] * nlayers,
+                eps_in=1.0, eps_out=2.085)
