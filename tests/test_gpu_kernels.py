@@ -59,3 +59,17 @@ def test_eig_batched_equals_single(ctx):
     for k in range(4):
         lam, W = ctx.eig(A[k])
         assert np.array_equal(lam, lam_b[k]) and np.array_equal(W, W_b[k])
+
+
+@pytest.mark.parametrize("n", [82, 98, 162])
+def test_zgemm_tiles_identical(ctx, n, monkeypatch):
+    """The 32 x 32 and 64 x 64 tiles accumulate every element over k in the
+    same order: their products agree bit for bit (so the engine's tile
+    autotuning cannot change results)."""
+    A, B = _rand(70, n), _rand(70, n)
+    out = {}
+    for tile in ("64", "32"):
+        monkeypatch.setenv("VRC_GEMM_TILE", tile)
+        out[tile] = ctx.zgemm(A, B)
+    assert np.array_equal(out["64"], out["32"])
+    assert relerr(out["32"], A @ B) < 1e-14

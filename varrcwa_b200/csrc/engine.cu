@@ -261,15 +261,59 @@ size_t Engine::batch_budget_bytes() const {
 // ---------------------------------------------------------------------------
 // Batched primitives
 // ---------------------------------------------------------------------------
+int Engine::gemm_tile_cached(int n, int opA, int opB) const {
+  auto it = gemm_tile_.find(n * 4 + opA * 2 + opB);
+  return it == gemm_tile_.end() ? 0 : it->second;
+}
+
+int Engine::gemm_tile(int n, int opA, int opB, size_t batch) {
+  if (const char* e = std::getenv("VRC_GEMM_TILE")) return std::atoi(e) == 32 ? 32 : 64;
+  if (n > 192) return 64;  // the 64-wide tile pads at most 25% there
+  const int key = n * 4 + opA * 2 + opB;
+  auto it = gemm_tile_.find(key);
+  if (it != gemm_tile_.end()) return it->second;
+  if (batch < 64) return 64;  // tune on a batch that fills the GPU
+  // time both tiles on zeroed scratch operands (a real call may update its
+  // output in place, so it cannot be run twice)
+  const int B = 128;
+  std::vector<cplx*> m3(3 * B);
+  for (auto& p : m3) {
+    p = mat(n);
+    VRC_CUDA_CHECK(cudaMemsetAsync(p, 0, (size_t)n * n * 16, stream_));
+  }
+  std::vector<GemmDesc> dd(B);
+  for (int b = 0; b < B; ++b) dd[b] = {m3[3 * b], m3[3 * b + 1], m3[3 * b + 2], nullptr, nullptr, nullptr};
+  GemmDesc* ddev = upload(dd);
+  cudaEvent_t ev[3];
+  for (auto& e : ev) VRC_CUDA_CHECK(cudaEventCreate(&e));
+  const int tiles[2] = {64, 32};
+  float ms[2] = {0.f, 0.f};
+  for (int t = 0; t < 2; ++t) {
+    zgemm_batched(ddev, B, n, mk(1, 0), mk(0, 0), 0.0, stream_, -1, opA, opB, tiles[t]);  // warm-up
+    VRC_CUDA_CHECK(cudaEventRecord(ev[0], stream_));
+    for (int r = 0; r < 3; ++r) zgemm_batched(ddev, B, n, mk(1, 0), mk(0, 0), 0.0, stream_, -1, opA, opB, tiles[t]);
+    VRC_CUDA_CHECK(cudaEventRecord(ev[1], stream_));
+    VRC_CUDA_CHECK(cudaEventSynchronize(ev[1]));
+    VRC_CUDA_CHECK(cudaEventElapsedTime(&ms[t], ev[0], ev[1]));
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  for (auto* p : m3) free_mat(p, n);
+  launches += 8;
+  const int best = ms[1] < ms[0] ? 32 : 64;
+  gemm_tile_[key] = best;
+  return best;
+}
+
 void Engine::gemm(std::vector<GemmDesc>& d, int n, cplx alpha, cplx beta, double delta, int opA, int opB) {
   if (d.empty()) return;
+  const int tile = gemm_tile(n, opA, opB, d.size());
   const size_t per = 16384;
   for (size_t b0 = 0; b0 < d.size(); b0 += per) {
     size_t nb = std::min(per, d.size() - b0);
     GemmDesc* dd = upload(d.data() + b0, nb);
     const double nn3 = (double)n * n * n;
     Prof pr(*this, "zgemm", 8.0 * nn3 * nb, 48.0 * n * (double)n * nb);
-    zgemm_batched(dd, (int)nb, n, alpha, beta, delta, stream_, -1, opA, opB);
+    zgemm_batched(dd, (int)nb, n, alpha, beta, delta, stream_, -1, opA, opB, tile);
   }
 }
 

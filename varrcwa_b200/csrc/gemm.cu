@@ -7,8 +7,13 @@
 // inner dimension kdim != n (A is n x kdim, B is kdim x n) for the rank-kdim
 // updates of the blocked inversion.  Either operand may be taken as its
 // conjugate transpose (square operands only; used by the adjoint).  One CTA
-// computes a 64 x 64 complex tile; operands are staged through shared memory
-// by 16-byte cp.async copies in a 3-stage pipeline.  The complex product
+// computes a 64 x 64 complex tile (eight warps of 32 x 16), or a 32 x 32
+// tile (four warps of 16 x 16) for small orders, where 64-wide tiles would
+// mostly compute padding (n = 82: 41% of a 128 x 128 cover is useful, 73% of
+// 96 x 96).  Every output element accumulates over k in the same order with
+// either tile, so the choice does not change results; the engine times both
+// once per shape and keeps the faster.  Operands are staged through shared
+// memory by 16-byte cp.async copies in a 3-stage pipeline.  The complex product
 // uses three real products (P1 = Ar Br, P2 = Ai Bi, P3 = (Ar+Ai)(Br+Bi);
 // Cr = P1 - P2, Ci = P3 - P1 - P2), as cuBLAS Zgemm3m on the reference GPU
 // path (src/gpu/types.cuh:33): a quarter fewer tensor-core products than the
@@ -20,11 +25,22 @@ namespace vrc {
 
 namespace {
 
-constexpr int BM = 64, BN = 64, BK = 8, STAGES = 3;
-constexpr int LDA = BM + 2;  // complex elements per k-row of the A tile
-constexpr int LDB = BN + 2;
-constexpr int NTHREADS = 256;
-constexpr int SMEM_BYTES = STAGES * BK * (LDA + LDB) * 16;
+constexpr int BK = 8, STAGES = 3;
+
+// Tile shape: WM x WN warps, each MT m16 tiles by NT n8 tiles.
+template <int WM_, int WN_, int MT_, int NT_>
+struct Tile {
+  static constexpr int WM = WM_, WN = WN_, MT = MT_, NT = NT_;
+  static constexpr int BM = WM * MT * 16, BN = WN * NT * 8;
+  static constexpr int THREADS = WM * WN * 32;
+  static constexpr int LDA = BM + 2;  // complex elements per k-row of the A tile
+  static constexpr int LDB = BN + 2;
+  static constexpr int SMEM = STAGES * BK * (LDA + LDB) * 16;
+  static constexpr int LOADS_A = BM * BK / THREADS, LOADS_B = BN * BK / THREADS;
+  static_assert(BM * BK % THREADS == 0 && BN * BK % THREADS == 0, "tile loads");
+};
+using T64 = Tile<2, 4, 2, 2>;  // 64 x 64, 256 threads
+using T32 = Tile<2, 2, 1, 2>;  // 32 x 32, 128 threads
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -48,9 +64,11 @@ __device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, doubl
 // OPA / OPB: 0 = the operand as stored, 1 = its conjugate transpose.  A
 // transposed operand is staged with consecutive threads along its stored
 // columns (coalesced) and conjugated when fragments are read.
-template <int OPA, int OPB>
-__global__ void __launch_bounds__(NTHREADS, 2)
+template <class TL, int OPA, int OPB>
+__global__ void __launch_bounds__(TL::THREADS, 512 / TL::THREADS)
     zgemm_kernel(const GemmDesc* __restrict__ descs, int n, int kdim, cplx alpha, cplx beta, double delta) {
+  constexpr int BM = TL::BM, BN = TL::BN, LDA = TL::LDA, LDB = TL::LDB, MT = TL::MT, NT = TL::NT;
+  constexpr int NTHREADS = TL::THREADS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx* As = reinterpret_cast<cplx*>(smem_raw);        // [STAGES][BK][LDA]
   cplx* Bs = As + STAGES * BK * LDA;                    // [STAGES][BK][LDB]
@@ -62,7 +80,7 @@ __global__ void __launch_bounds__(NTHREADS, 2)
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
   const int g = lane >> 2, tig = lane & 3;
-  const int wm = warp & 1, wn = warp >> 1;  // 2 x 4 warps, 32 x 16 complex each
+  const int wm = warp % TL::WM, wn = warp / TL::WM;  // warp tile: MT*16 x NT*8 complex
 
   const cplx* __restrict__ A = d.A;
   const cplx* __restrict__ B = d.B;
@@ -73,11 +91,11 @@ __global__ void __launch_bounds__(NTHREADS, 2)
     cplx* as = As + stage * BK * LDA;
     cplx* bs = Bs + stage * BK * LDB;
 #pragma unroll
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < TL::LOADS_A; ++i) {
       int idx = tid + i * NTHREADS;
       if (OPA == 0) {
-        // A tile: 64 rows x 8 cols, consecutive threads -> consecutive rows.
-        int r = idx & 63, k = idx >> 6;
+        // A tile: BM rows x 8 cols, consecutive threads -> consecutive rows.
+        int r = idx % BM, k = idx / BM;
         int gr = m0 + r, gk = k0 + k;
         bool va = (gr < n) && (gk < kdim);
         cp_async16(as + k * LDA + r, va ? (const void*)(A + (size_t)gk * n + gr) : (const void*)A, va);
@@ -88,15 +106,19 @@ __global__ void __launch_bounds__(NTHREADS, 2)
         bool va = (gr < n) && (gk < kdim);
         cp_async16(as + k * LDA + r, va ? (const void*)(A + (size_t)gr * n + gk) : (const void*)A, va);
       }
+    }
+#pragma unroll
+    for (int i = 0; i < TL::LOADS_B; ++i) {
+      int idx = tid + i * NTHREADS;
       if (OPB == 0) {
-        // B tile: 8 rows x 64 cols, consecutive threads -> consecutive k.
+        // B tile: 8 rows x BN cols, consecutive threads -> consecutive k.
         int kb = idx & 7, c = idx >> 3;
         int gkb = k0 + kb, gc = n0 + c;
         bool vb = (gkb < kdim) && (gc < n);
         cp_async16(bs + kb * LDB + c, vb ? (const void*)(B + (size_t)gc * kdim + gkb) : (const void*)B, vb);
       } else {
         // op(B)(k, c) = conj(B(c, k)), stored at B[k * n + c]: threads along c.
-        int c = idx & 63, kb = idx >> 6;
+        int c = idx % BN, kb = idx / BN;
         int gkb = k0 + kb, gc = n0 + c;
         bool vb = (gkb < kdim) && (gc < n);
         cp_async16(bs + kb * LDB + c, vb ? (const void*)(B + (size_t)gkb * n + gc) : (const void*)B, vb);
@@ -104,11 +126,11 @@ __global__ void __launch_bounds__(NTHREADS, 2)
     }
   };
 
-  double acc1[2][2][4], acc2[2][2][4], acc3[2][2][4];
+  double acc1[MT][NT][4], acc2[MT][NT][4], acc3[MT][NT][4];
 #pragma unroll
-  for (int a = 0; a < 2; ++a)
+  for (int a = 0; a < MT; ++a)
 #pragma unroll
-    for (int b = 0; b < 2; ++b)
+    for (int b = 0; b < NT; ++b)
 #pragma unroll
       for (int c = 0; c < 4; ++c) acc1[a][b][c] = acc2[a][b][c] = acc3[a][b][c] = 0.0;
 
@@ -129,10 +151,10 @@ __global__ void __launch_bounds__(NTHREADS, 2)
     const cplx* bs = Bs + (kt % STAGES) * BK * LDB;
 #pragma unroll
     for (int ks = 0; ks < BK; ks += 4) {
-      cplx af[2][2], bf[2];
+      cplx af[MT][2], bf[NT];
 #pragma unroll
-      for (int mt = 0; mt < 2; ++mt) {
-        int row = wm * 32 + mt * 16 + g;
+      for (int mt = 0; mt < MT; ++mt) {
+        int row = wm * (MT * 16) + mt * 16 + g;
         af[mt][0] = as[(ks + tig) * LDA + row];
         af[mt][1] = as[(ks + tig) * LDA + row + 8];
         if (OPA) {
@@ -141,14 +163,14 @@ __global__ void __launch_bounds__(NTHREADS, 2)
         }
       }
 #pragma unroll
-      for (int nt = 0; nt < 2; ++nt) {
-        bf[nt] = bs[(ks + tig) * LDB + wn * 16 + nt * 8 + g];
+      for (int nt = 0; nt < NT; ++nt) {
+        bf[nt] = bs[(ks + tig) * LDB + wn * (NT * 8) + nt * 8 + g];
         if (OPB) bf[nt].y = -bf[nt].y;
       }
 #pragma unroll
-      for (int mt = 0; mt < 2; ++mt)
+      for (int mt = 0; mt < MT; ++mt)
 #pragma unroll
-        for (int nt = 0; nt < 2; ++nt) {
+        for (int nt = 0; nt < NT; ++nt) {
           dmma(acc1[mt][nt], af[mt][0].x, af[mt][1].x, bf[nt].x);
           dmma(acc2[mt][nt], af[mt][0].y, af[mt][1].y, bf[nt].y);
           dmma(acc3[mt][nt], af[mt][0].x + af[mt][0].y, af[mt][1].x + af[mt][1].y, bf[nt].x + bf[nt].y);
@@ -159,13 +181,13 @@ __global__ void __launch_bounds__(NTHREADS, 2)
 
   // Epilogue.
 #pragma unroll
-  for (int mt = 0; mt < 2; ++mt)
+  for (int mt = 0; mt < MT; ++mt)
 #pragma unroll
-    for (int nt = 0; nt < 2; ++nt)
+    for (int nt = 0; nt < NT; ++nt)
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
-        int row = m0 + wm * 32 + mt * 16 + g + ((c >> 1) << 3);
-        int col = n0 + wn * 16 + nt * 8 + tig * 2 + (c & 1);
+        int row = m0 + wm * (MT * 16) + mt * 16 + g + ((c >> 1) << 3);
+        int col = n0 + wn * (NT * 8) + nt * 8 + tig * 2 + (c & 1);
         if (row < n && col < n) {
           const double p1 = acc1[mt][nt][c], p2 = acc2[mt][nt][c];
           cplx v = mk(p1 - p2, acc3[mt][nt][c] - p1 - p2);
@@ -180,32 +202,39 @@ __global__ void __launch_bounds__(NTHREADS, 2)
       }
 }
 
-}  // namespace
-
-void zgemm_batched(const GemmDesc* d_descs, int batch, int n, cplx alpha, cplx beta, double delta,
-                   cudaStream_t stream, int kdim, int opA, int opB) {
-  if (kdim < 0) kdim = n;
-  if ((opA || opB) && kdim != n) throw StatusError(ST_EINVAL, "transposed GEMM operands must be square");
+template <class TL>
+void launch_tile(const GemmDesc* d_descs, int batch, int n, cplx alpha, cplx beta, double delta,
+                 cudaStream_t stream, int kdim, int opA, int opB) {
   static bool configured = false;
   if (!configured) {
-    VRC_CUDA_CHECK(cudaFuncSetAttribute(zgemm_kernel<0, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        SMEM_BYTES));
-    VRC_CUDA_CHECK(cudaFuncSetAttribute(zgemm_kernel<1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        SMEM_BYTES));
-    VRC_CUDA_CHECK(cudaFuncSetAttribute(zgemm_kernel<0, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        SMEM_BYTES));
-    VRC_CUDA_CHECK(cudaFuncSetAttribute(zgemm_kernel<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        SMEM_BYTES));
+    VRC_CUDA_CHECK(cudaFuncSetAttribute(zgemm_kernel<TL, 0, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, TL::SMEM));
+    VRC_CUDA_CHECK(cudaFuncSetAttribute(zgemm_kernel<TL, 1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, TL::SMEM));
+    VRC_CUDA_CHECK(cudaFuncSetAttribute(zgemm_kernel<TL, 0, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, TL::SMEM));
+    VRC_CUDA_CHECK(cudaFuncSetAttribute(zgemm_kernel<TL, 1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, TL::SMEM));
     configured = true;
   }
-  if (batch <= 0) return;
-  auto kern = opA ? (opB ? zgemm_kernel<1, 1> : zgemm_kernel<1, 0>) : (opB ? zgemm_kernel<0, 1> : zgemm_kernel<0, 0>);
-  int tiles = ((n + BM - 1) / BM) * ((n + BN - 1) / BN);
+  auto kern = opA ? (opB ? zgemm_kernel<TL, 1, 1> : zgemm_kernel<TL, 1, 0>)
+                  : (opB ? zgemm_kernel<TL, 0, 1> : zgemm_kernel<TL, 0, 0>);
+  const int tiles = ((n + TL::BM - 1) / TL::BM) * ((n + TL::BN - 1) / TL::BN);
   for (int b0 = 0; b0 < batch; b0 += 65535) {
     int nb = batch - b0 < 65535 ? batch - b0 : 65535;
     dim3 grid(tiles, nb);
-    kern<<<grid, NTHREADS, SMEM_BYTES, stream>>>(d_descs + b0, n, kdim, alpha, beta, delta);
+    kern<<<grid, TL::THREADS, TL::SMEM, stream>>>(d_descs + b0, n, kdim, alpha, beta, delta);
   }
+}
+
+}  // namespace
+
+void zgemm_batched(const GemmDesc* d_descs, int batch, int n, cplx alpha, cplx beta, double delta,
+                   cudaStream_t stream, int kdim, int opA, int opB, int tile) {
+  if (kdim < 0) kdim = n;
+  if ((opA || opB) && kdim != n) throw StatusError(ST_EINVAL, "transposed GEMM operands must be square");
+  if (tile != 32 && tile != 64) throw StatusError(ST_EINVAL, "GEMM tile must be 32 or 64");
+  if (batch <= 0) return;
+  if (tile == 32)
+    launch_tile<T32>(d_descs, batch, n, alpha, beta, delta, stream, kdim, opA, opB);
+  else
+    launch_tile<T64>(d_descs, batch, n, alpha, beta, delta, stream, kdim, opA, opB);
   VRC_CUDA_CHECK(cudaGetLastError());
 }
 

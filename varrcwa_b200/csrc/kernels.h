@@ -16,8 +16,9 @@ struct GemmDesc {
   const cplx* cs;   // optional column scale (n)
 };
 // opA / opB = 1 takes that operand as its conjugate transpose (kdim == n).
+// tile: 64 (64 x 64 complex per CTA) or 32 (32 x 32); results are identical.
 void zgemm_batched(const GemmDesc* d_descs, int batch, int n, cplx alpha, cplx beta, double delta,
-                   cudaStream_t stream, int kdim = -1, int opA = 0, int opB = 0);  // kdim < 0: n
+                   cudaStream_t stream, int kdim = -1, int opA = 0, int opB = 0, int tile = 64);  // kdim < 0: n
 
 // ---- inverse (in place) -------------------------------------------------------
 int zinv_panel_width(int n);
