@@ -216,13 +216,17 @@ int vrc_stack_backward(vrc_context* ctx, const double* wR, const double* wT, dou
 
 /* ---- instrumentation (no counterpart in the reference) ---------------------
  * Per-kernel-family device time measured with CUDA events on the engine
- * stream, with the algorithmic FP64 flops and bytes of the timed launches. */
+ * streams, with the algorithmic FP64 flops and bytes of the timed launches.
+ * ms sums the launches' durations; busy_ms is the length of the union of
+ * their intervals (they overlap when a call's cells are solved on several
+ * concurrent engines). */
 typedef struct {
   char name[32];
   double ms;
   long long launches;
   double flops;
   double bytes;
+  double busy_ms;
 } vrc_kernel_stat;
 int vrc_set_profiling(vrc_context* ctx, int enable); /* also resets the counters */
 /* Returns the number of families (fills at most max entries of out). */

@@ -110,3 +110,23 @@ def test_invalid_arguments_are_rejected(ctx):
     assert e.value.status == 1
     with pytest.raises(VrcError):
         ctx.redheffer([CASES["asym_redheffer"]["desc"]], pe=-1.0)
+
+
+def test_lanes_match_one_engine(ctx, monkeypatch):
+    """A call on many cells is split over concurrent engines (lanes); every
+    cell's arithmetic is the same as on one engine, so results agree bit for
+    bit, in call order, with the trees kept per cell."""
+    from varrcwa_b200 import structures as st
+    cells = [st.pillar_cell(2100 + i, norders=3, lam=0.532, npix=32) for i in range(8)]
+    out = {}
+    for lanes in ("1", "3"):
+        monkeypatch.setenv("VRC_LANES", lanes)
+        out[lanes] = (ctx.order_powers(cells, method="redheffer", pe=1e-2, side=1),
+                      ctx.redheffer(cells, pe=1e-2), [ctx.tree(c) for c in range(len(cells))])
+    for a, b in zip(out["1"][0], out["3"][0]):
+        assert np.array_equal(a["R"], b["R"]) and np.array_equal(a["T"], b["T"])
+    for a, b in zip(out["1"][1], out["3"][1]):
+        for k in ("Tdd", "Tuu", "Rud", "Rdu"):
+            assert np.array_equal(a[k], b[k])
+        assert a["N"] == b["N"]
+    assert out["1"][2] == out["3"][2]

@@ -75,7 +75,7 @@ class VrcTiming(C.Structure):
 
 class VrcKernelStat(C.Structure):
     _fields_ = [("name", C.c_char * 32), ("ms", C.c_double), ("launches", C.c_longlong), ("flops", C.c_double),
-                ("bytes", C.c_double)]
+                ("bytes", C.c_double), ("busy_ms", C.c_double)]
 
 
 class VrcError(RuntimeError):
@@ -244,7 +244,7 @@ class Context:
         arr = (VrcKernelStat * max(cnt, 1))()
         self.L.vrc_get_kernel_stats(self.h, cnt, arr)
         return {arr[i].name.decode(): {"ms": arr[i].ms, "launches": int(arr[i].launches), "flops": arr[i].flops,
-                                       "bytes": arr[i].bytes} for i in range(cnt)}
+                                       "bytes": arr[i].bytes, "busy_ms": arr[i].busy_ms} for i in range(cnt)}
 
     # ---- assembly / eigen ----
     def sample_pq(self, desc: dict, zs: Sequence[float]):

@@ -535,7 +535,7 @@ void pixel_adjoint_batched(const PixAdjDesc* d, int batch, int nx, int ny, int n
   if (!pixel_adjoint_fits(nx, ny, npx, npy))
     throw StatusError(ST_EINVAL, "pixel adjoint: raster and harmonics exceed the shared-memory tile");
   const size_t smem = pixel_adjoint_smem(nx, ny, npx, npy);
-  VRC_CUDA_CHECK(cudaFuncSetAttribute(pixel_adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  ensure_smem((const void*)pixel_adjoint_kernel, smem);
   pixel_adjoint_kernel<<<batch, PX_THREADS, smem, st>>>(d, nx, ny, npx, npy);
   VRC_CUDA_CHECK(cudaGetLastError());
 }
@@ -544,7 +544,7 @@ void stack_power_batched(const StackPowerDesc* d, int batch, int m, int adj, cud
   if (batch <= 0) return;
   const size_t smem = (size_t)7 * 2 * m * 16;
   if (smem > 227 * 1024) throw StatusError(ST_EINVAL, "stack powers: n too large");
-  VRC_CUDA_CHECK(cudaFuncSetAttribute(stack_power_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  ensure_smem((const void*)stack_power_kernel, smem);
   stack_power_kernel<<<batch, 256, smem, st>>>(d, m, adj);
   VRC_CUDA_CHECK(cudaGetLastError());
 }

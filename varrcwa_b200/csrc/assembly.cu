@@ -339,11 +339,7 @@ void toeplitz_inverses(const cplx* const* d_F, cplx* const* d_out, int t, int nm
   const size_t per_warp = (size_t)(t * t + t) * 16 + TI_MAXT * sizeof(int);
   int nw = (int)std::min<size_t>(TI_WARPS, std::max<size_t>(1, (200u << 10) / per_warp));
   size_t smem = per_warp * nw;
-  static size_t configured = 0;
-  if (smem > 48 * 1024 && smem > configured) {
-    VRC_CUDA_CHECK(cudaFuncSetAttribute(toeplitz_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    configured = smem;
-  }
+  ensure_smem((const void*)toeplitz_inv_kernel, smem);
   dim3 grid((nmat + nw - 1) / nw, batch);
   toeplitz_inv_kernel<<<grid, nw * 32, smem, st>>>(d_F, d_out, t, nmat, d_status);
   VRC_CUDA_CHECK(cudaGetLastError());

@@ -6,11 +6,17 @@
 #include <algorithm>
 #include <chrono>
 #include <cstring>
+#include <exception>
 #include <memory>
 #include <string>
+#include <thread>
 
 struct vrc_context {
   std::unique_ptr<vrc::Engine> eng;
+  // further engines ("lanes") that solve groups of a call's cells
+  // concurrently, each with its own stream, memory pools and host thread
+  std::vector<std::unique_ptr<vrc::Engine>> lanes;
+  cudaEvent_t origin = nullptr;  // time origin of the profiled launch intervals
   std::string err;
   vrc_timing timing{0.0, 0};
   std::vector<std::vector<vrc::NodeRecord>> trees;
@@ -43,10 +49,16 @@ int guarded(vrc_context* ctx, F&& f) {
   }
 }
 
+long long all_launches(const vrc_context* ctx) {
+  long long l = ctx->eng->launches;
+  for (auto& e : ctx->lanes) l += e->launches;
+  return l;
+}
+
 struct Timed {
   vrc_context* ctx;
   long long l0;
-  explicit Timed(vrc_context* c) : ctx(c), l0(c->eng->launches) {
+  explicit Timed(vrc_context* c) : ctx(c), l0(all_launches(c)) {
     VRC_CUDA_CHECK(cudaEventRecord(ctx->ev0, ctx->eng->stream()));
     c->eng->bubble_ms_ = c->eng->sync_ms_ = 0.0;
     c->eng->nsync_ = 0;
@@ -75,7 +87,7 @@ struct Timed {
     float ms = 0.f;
     VRC_CUDA_CHECK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
     ctx->timing.device_ms = ms;
-    ctx->timing.launches = ctx->eng->launches - l0;
+    ctx->timing.launches = all_launches(ctx) - l0;
   }
 };
 
@@ -153,11 +165,92 @@ void d2h(void* dst, const void* src, size_t bytes, cudaStream_t st) {
   if (dst && src) VRC_CUDA_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
 }
 
-void export_results(vrc_context* ctx, std::vector<vrc::CellResult>& res, vrc_result* out) {
-  vrc::Engine& E = *ctx->eng;
+vrc::Engine& lane(vrc_context* ctx, int g) { return g == 0 ? *ctx->eng : *ctx->lanes[g - 1]; }
+
+// Lanes for a call on ncells cells: three when every lane gets at least two
+// cells (measured: 128 config-2 cells solve 10% faster on three lanes than
+// on one, as one lane's partly filled kernel waves overlap another's work),
+// else one; VRC_LANES (1..8) overrides.
+int lane_count(int ncells) {
+  int g = ncells >= 6 ? 3 : 1;
+  if (const char* e = std::getenv("VRC_LANES")) g = std::atoi(e);
+  return std::max(1, std::min({g, 8, std::max(ncells, 1)}));
+}
+
+// Deals the cells round-robin over the lanes and runs
+// solve(lane index, engine, cells, their indices in the call, results) on
+// every lane in its own host thread.  Results come back in call order with
+// the lane that owns each one (its device blocks live in that engine).
+template <class F>
+void run_lanes(vrc_context* ctx, const std::vector<vrc::CellSpec>& specs, std::vector<vrc::CellResult>& res,
+               std::vector<int>& owner, F&& solve) {
+  const int C = (int)specs.size();
+  const int G = lane_count(C);
+  while ((int)ctx->lanes.size() < G - 1) {
+    auto e = std::make_unique<vrc::Engine>(ctx->eng->device());
+    e->set_profiling(ctx->eng->profiling());
+    e->set_time_origin(ctx->origin);
+    ctx->lanes.push_back(std::move(e));
+  }
+  std::vector<std::vector<vrc::CellSpec>> gs(G);
+  std::vector<std::vector<int>> ids(G);
+  for (int c = 0; c < C; ++c) {
+    gs[c % G].push_back(specs[c]);
+    ids[c % G].push_back(c);
+  }
+  std::vector<std::vector<vrc::CellResult>> out(G);
+  for (int g = 1; g < G; ++g)  // lane work starts after the call's first event
+    VRC_CUDA_CHECK(cudaStreamWaitEvent(lane(ctx, g).stream(), ctx->ev0, 0));
+  std::vector<std::exception_ptr> err(G);
+  std::vector<std::thread> th;
+  const int dev = ctx->eng->device();
+  for (int g = 1; g < G; ++g)
+    th.emplace_back([&, g] {
+      try {
+        VRC_CUDA_CHECK(cudaSetDevice(dev));
+        solve(g, lane(ctx, g), gs[g], ids[g], out[g]);
+      } catch (...) {
+        err[g] = std::current_exception();
+      }
+    });
+  try {
+    solve(0, *ctx->eng, gs[0], ids[0], out[0]);
+  } catch (...) {
+    err[0] = std::current_exception();
+  }
+  for (auto& t : th) t.join();
+  for (int g = 0; g < G; ++g)
+    if (err[g]) {
+      for (int h = 0; h < G; ++h) {
+        lane(ctx, h).sync();
+        for (auto& r : out[h]) lane(ctx, h).release_result(r);
+      }
+      std::rethrow_exception(err[g]);
+    }
+  // the context's stream waits for every lane, so the call's device time
+  // spans all of them
+  for (int g = 1; g < G; ++g) {
+    cudaEvent_t ev;
+    VRC_CUDA_CHECK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    VRC_CUDA_CHECK(cudaEventRecord(ev, lane(ctx, g).stream()));
+    VRC_CUDA_CHECK(cudaStreamWaitEvent(ctx->eng->stream(), ev, 0));
+    VRC_CUDA_CHECK(cudaEventDestroy(ev));
+  }
+  res.assign(C, vrc::CellResult());
+  owner.assign(C, 0);
+  for (int g = 0; g < G; ++g)
+    for (size_t k = 0; k < ids[g].size(); ++k) {
+      res[ids[g][k]] = out[g][k];
+      owner[ids[g][k]] = g;
+    }
+}
+
+void export_results(vrc_context* ctx, std::vector<vrc::CellResult>& res, const std::vector<int>& owner,
+                    vrc_result* out) {
   ctx->trees.clear();
   for (size_t c = 0; c < res.size(); ++c) {
     vrc::CellResult& r = res[c];
+    vrc::Engine& E = lane(ctx, owner[c]);
     const size_t nn = (size_t)r.n * r.n * 16, nv = (size_t)r.n * 16;
     if (out) {
       vrc_result& o = out[c];
@@ -180,8 +273,9 @@ void export_results(vrc_context* ctx, std::vector<vrc::CellResult>& res, vrc_res
     }
     ctx->trees.push_back(r.nodes);
   }
-  E.sync();
-  for (auto& r : res) E.release_result(r);
+  ctx->eng->sync();
+  for (auto& e : ctx->lanes) e->sync();
+  for (size_t c = 0; c < res.size(); ++c) lane(ctx, owner[c]).release_result(res[c]);
 }
 }  // namespace
 
@@ -212,6 +306,8 @@ int vrc_create(int device, vrc_context** ctx) {
 void vrc_destroy(vrc_context* ctx) {
   if (!ctx) return;
   if (ctx->eng) cudaSetDevice(ctx->eng->device());
+  ctx->lanes.clear();
+  if (ctx->origin) cudaEventDestroy(ctx->origin);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   ctx->eng.reset();
@@ -331,10 +427,13 @@ int vrc_redheffer(vrc_context* ctx, int ncells, const vrc_cell* cells, double pe
     o.pe = pe;
     o.max_depth = max_depth;
     std::vector<vrc::CellResult> res;
+    std::vector<int> owner;
     Timed tm(ctx);
-    ctx->eng->redheffer(specs, o, res);
+    run_lanes(ctx, specs, res, owner,
+              [&](int, vrc::Engine& E, const std::vector<vrc::CellSpec>& sp, const std::vector<int>&,
+                  std::vector<vrc::CellResult>& r) { E.redheffer(sp, o, r); });
     tm.done();
-    export_results(ctx, res, results);
+    export_results(ctx, res, owner, results);
   });
 }
 
@@ -352,13 +451,20 @@ int vrc_redheffer_segments(vrc_context* ctx, int ncells, const vrc_cell* cells, 
       specs[c].z0 = cv[c].front();
       specs[c].z1 = cv[c].back();
     }
-    vrc::Engine::RedhefferOpts o;
-    o.cuts = &cv;
     std::vector<vrc::CellResult> res;
+    std::vector<int> owner;
     Timed tm(ctx);
-    ctx->eng->redheffer(specs, o, res);
+    run_lanes(ctx, specs, res, owner,
+              [&](int, vrc::Engine& E, const std::vector<vrc::CellSpec>& sp, const std::vector<int>& ids,
+                  std::vector<vrc::CellResult>& r) {
+                std::vector<std::vector<double>> lc;
+                for (int c : ids) lc.push_back(cv[c]);
+                vrc::Engine::RedhefferOpts o;
+                o.cuts = &lc;
+                E.redheffer(sp, o, r);
+              });
     tm.done();
-    export_results(ctx, res, results);
+    export_results(ctx, res, owner, results);
   });
 }
 
@@ -378,10 +484,13 @@ int vrc_rcwa(vrc_context* ctx, int ncells, const vrc_cell* cells, int N, vrc_res
   return guarded(ctx, [&] {
     auto specs = to_specs(ncells, cells);
     std::vector<vrc::CellResult> res;
+    std::vector<int> owner;
     Timed tm(ctx);
-    ctx->eng->rcwa(specs, N, res);
+    run_lanes(ctx, specs, res, owner,
+              [&](int, vrc::Engine& E, const std::vector<vrc::CellSpec>& sp, const std::vector<int>&,
+                  std::vector<vrc::CellResult>& r) { E.rcwa(sp, N, r); });
     tm.done();
-    export_results(ctx, res, results);
+    export_results(ctx, res, owner, results);
   });
 }
 
@@ -389,10 +498,13 @@ int vrc_differential(vrc_context* ctx, int ncells, const vrc_cell* cells, int N,
   return guarded(ctx, [&] {
     auto specs = to_specs(ncells, cells);
     std::vector<vrc::CellResult> res;
+    std::vector<int> owner;
     Timed tm(ctx);
-    ctx->eng->differential(specs, N, res);
+    run_lanes(ctx, specs, res, owner,
+              [&](int, vrc::Engine& E, const std::vector<vrc::CellSpec>& sp, const std::vector<int>&,
+                  std::vector<vrc::CellResult>& r) { E.differential(sp, N, r); });
     tm.done();
-    export_results(ctx, res, results);
+    export_results(ctx, res, owner, results);
   });
 }
 
@@ -401,24 +513,32 @@ int vrc_order_powers(vrc_context* ctx, int ncells, const vrc_cell* cells, int me
   return guarded(ctx, [&] {
     if (!R || !T || (side != 0 && side != 1)) throw vrc::StatusError(VRC_EINVAL, "invalid arguments");
     auto specs = to_specs(ncells, cells);
-    vrc::Engine& E = *ctx->eng;
+    if (method < 0 || method > 2) throw vrc::StatusError(VRC_EINVAL, "unknown method");
+    if (method == 0 && !(pe > 0.0)) throw vrc::StatusError(VRC_EINVAL, "pe must be > 0");
     std::vector<vrc::CellResult> res;
+    std::vector<int> owner;
+    std::vector<std::vector<double>> Rv(ncells), Tv(ncells);
     Timed tm(ctx);
-    if (method == 0) {
-      if (!(pe > 0.0)) throw vrc::StatusError(VRC_EINVAL, "pe must be > 0");
-      vrc::Engine::RedhefferOpts o;
-      o.pe = pe;
-      o.max_depth = max_depth;
-      E.redheffer(specs, o, res);
-    } else if (method == 1) {
-      E.rcwa(specs, nslices, res);
-    } else if (method == 2) {
-      E.differential(specs, nslices, res);
-    } else {
-      throw vrc::StatusError(VRC_EINVAL, "unknown method");
-    }
-    std::vector<std::vector<double>> Rv, Tv;
-    E.order_powers(specs, res, side, flux_norm, Rv, Tv);
+    run_lanes(ctx, specs, res, owner,
+              [&](int, vrc::Engine& E, const std::vector<vrc::CellSpec>& sp, const std::vector<int>& ids,
+                  std::vector<vrc::CellResult>& r) {
+                if (method == 0) {
+                  vrc::Engine::RedhefferOpts o;
+                  o.pe = pe;
+                  o.max_depth = max_depth;
+                  E.redheffer(sp, o, r);
+                } else if (method == 1) {
+                  E.rcwa(sp, nslices, r);
+                } else {
+                  E.differential(sp, nslices, r);
+                }
+                std::vector<std::vector<double>> lr, lt;
+                E.order_powers(sp, r, side, flux_norm, lr, lt);
+                for (size_t k = 0; k < ids.size(); ++k) {
+                  Rv[ids[k]] = std::move(lr[k]);
+                  Tv[ids[k]] = std::move(lt[k]);
+                }
+              });
     tm.done();
     size_t off = 0;
     for (int c = 0; c < ncells; ++c) {
@@ -428,9 +548,9 @@ int vrc_order_powers(vrc_context* ctx, int ncells, const vrc_cell* cells, int me
       if (status) status[c] = res[c].status;
     }
     ctx->trees.clear();
-    for (auto& r : res) {
-      ctx->trees.push_back(r.nodes);
-      E.release_result(r);
+    for (int c = 0; c < ncells; ++c) {
+      ctx->trees.push_back(res[c].nodes);
+      lane(ctx, owner[c]).release_result(res[c]);
     }
   });
 }
@@ -471,6 +591,17 @@ int vrc_set_profiling(vrc_context* ctx, int enable) {
   return guarded(ctx, [&] {
     ctx->eng->set_profiling(enable != 0);
     ctx->eng->reset_fam_stats();
+    for (auto& e : ctx->lanes) {
+      e->set_profiling(enable != 0);
+      e->reset_fam_stats();
+    }
+    if (!ctx->origin) VRC_CUDA_CHECK(cudaEventCreate(&ctx->origin));
+    VRC_CUDA_CHECK(cudaEventRecord(ctx->origin, ctx->eng->stream()));
+    ctx->eng->set_time_origin(ctx->origin);
+    for (auto& e : ctx->lanes) {
+      VRC_CUDA_CHECK(cudaStreamWaitEvent(e->stream(), ctx->origin, 0));
+      e->set_time_origin(ctx->origin);
+    }
   });
 }
 
@@ -478,7 +609,18 @@ int vrc_get_kernel_stats(vrc_context* ctx, int max, vrc_kernel_stat* out) {
   if (!ctx) return -VRC_EINVAL;
   int count = 0;
   int st = guarded(ctx, [&] {
-    auto& f = ctx->eng->fam_stats();
+    // summed over the lanes: with concurrent lanes a family's time is the
+    // sum of its launches' durations, each measured on its own stream
+    std::map<std::string, vrc::Engine::FamStat> f = ctx->eng->fam_stats();
+    for (auto& e : ctx->lanes)
+      for (auto& kv : e->fam_stats()) {
+        auto& d = f[kv.first];
+        d.ms += kv.second.ms;
+        d.launches += kv.second.launches;
+        d.flops += kv.second.flops;
+        d.bytes += kv.second.bytes;
+        d.iv.insert(d.iv.end(), kv.second.iv.begin(), kv.second.iv.end());
+      }
     for (auto& kv : f) {
       if (out && count < max) {
         vrc_kernel_stat& o = out[count];
@@ -488,6 +630,20 @@ int vrc_get_kernel_stats(vrc_context* ctx, int max, vrc_kernel_stat* out) {
         o.launches = kv.second.launches;
         o.flops = kv.second.flops;
         o.bytes = kv.second.bytes;
+        auto iv = kv.second.iv;  // union of the launch intervals
+        std::sort(iv.begin(), iv.end());
+        double busy = 0.0, s0 = 0.0, s1 = -1.0;
+        for (auto& p : iv) {
+          if (p.first > s1) {
+            if (s1 > s0) busy += s1 - s0;
+            s0 = p.first;
+            s1 = p.second;
+          } else if (p.second > s1) {
+            s1 = p.second;
+          }
+        }
+        if (s1 > s0) busy += s1 - s0;
+        o.busy_ms = iv.empty() ? kv.second.ms : busy;
       }
       ++count;
     }

@@ -266,12 +266,7 @@ __global__ void vecnorm_kernel(cplx* const* __restrict__ Xs, int n) {
 template <int NT>
 void launch_hess(cplx* const* H, cplx* const* Z, int batch, int n, cudaStream_t st) {
   size_t smem = (size_t)(4 + HESS_WARPS) * n * 16;
-  static size_t configured = 0;
-  if (smem > 48 * 1024 && smem > configured) {
-    VRC_CUDA_CHECK(cudaFuncSetAttribute(hess_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)smem));
-    configured = smem;
-  }
+  ensure_smem((const void*)hess_kernel<NT>, smem);
   for (int b0 = 0; b0 < batch; b0 += 65535) {
     int nb = min(65535, batch - b0);
     hess_kernel<NT><<<nb, HESS_THREADS, smem, st>>>(H + b0, Z + b0, n);
@@ -290,12 +285,12 @@ void hessenberg_batched(cplx* const* d_H, cplx* const* d_Z, int batch, int n, cu
   // SM two matrices; the cluster kernel wins for 192 < n <= 256 at every batch
   // (matrix in shared memory) and for n >= 400, where the single-CTA
   // reduction's per-matrix latency dominates.
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
+  static const int sms = [] {
+    int dev = 0, v = 0;
     VRC_CUDA_CHECK(cudaGetDevice(&dev));
-    VRC_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  }
+    VRC_CUDA_CHECK(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
+    return v;
+  }();
   const bool full = batch >= 2 * sms;
   const bool cluster = hessenberg_cluster_fits(n) && n > 128 &&
                        ((n > 192 && n <= 256) || n >= 400 || !full);
@@ -313,11 +308,7 @@ void hessenberg_batched(cplx* const* d_H, cplx* const* d_Z, int batch, int n, cu
 void trevc_batched(cplx* const* d_T, cplx* const* d_Y, int batch, int n, cudaStream_t st) {
   if (batch <= 0) return;
   size_t smem = (size_t)TV_WARPS * n * 16;
-  static size_t configured = 0;
-  if (smem > 48 * 1024 && smem > configured) {
-    VRC_CUDA_CHECK(cudaFuncSetAttribute(trevc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    configured = smem;
-  }
+  ensure_smem((const void*)trevc_kernel, smem);
   for (int b0 = 0; b0 < batch; b0 += 65535) {
     int nb = min(65535, batch - b0);
     dim3 grid((n + TV_WARPS - 1) / TV_WARPS, nb);

@@ -5,6 +5,7 @@
 #include "engine.h"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <complex>
@@ -12,6 +13,7 @@
 #include <cstring>
 #include <tuple>
 #include <list>
+#include <mutex>
 #include <numeric>
 #include <stdexcept>
 
@@ -59,12 +61,13 @@ BlockPool::~BlockPool() {
 }
 
 namespace {
-double g_host_alloc_ms = 0.0;  // host time spent in cudaMalloc/cudaFree
+// host time spent in cudaMalloc/cudaFree (all engines), in microseconds
+std::atomic<long long> g_host_alloc_us{0};
 struct AllocTimer {
   std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
   ~AllocTimer() {
-    g_host_alloc_ms +=
-        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    g_host_alloc_us += (long long)std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0)
+                           .count();
   }
 };
 }  // namespace
@@ -148,6 +151,12 @@ void Engine::resolve_prof() {
     VRC_CUDA_CHECK(cudaEventElapsedTime(&ms, p.a, p.b));
     FamStat& f = fam_[p.fam];
     f.ms += ms;
+    if (origin_) {  // the launch's interval on the time line shared by all engines
+      float t0 = 0.f, t1 = 0.f;
+      VRC_CUDA_CHECK(cudaEventElapsedTime(&t0, origin_, p.a));
+      VRC_CUDA_CHECK(cudaEventElapsedTime(&t1, origin_, p.b));
+      f.iv.push_back({t0, t1});
+    }
     f.launches += p.nl;
     f.flops += p.flops;
     f.bytes += p.bytes;
@@ -172,13 +181,13 @@ void Engine::set_profiling(bool on) {
 }
 std::map<std::string, Engine::FamStat>& Engine::fam_stats() {
   sync();
-  fam_["host_alloc"].ms = g_host_alloc_ms - alloc_ms0_;
+  fam_["host_alloc"].ms = 1e-3 * (double)g_host_alloc_us.load() - alloc_ms0_;
   return fam_;
 }
 void Engine::reset_fam_stats() {
   sync();
   fam_.clear();
-  alloc_ms0_ = g_host_alloc_ms;
+  alloc_ms0_ = 1e-3 * (double)g_host_alloc_us.load();
 }
 
 Engine::Prof::Prof(Engine& eng, const char* f, double fl, double by, int nlaunch)
@@ -261,6 +270,18 @@ size_t Engine::batch_budget_bytes() const {
 // ---------------------------------------------------------------------------
 // Batched primitives
 // ---------------------------------------------------------------------------
+void ensure_smem(const void* kernel, size_t bytes) {
+  if (bytes <= 48 * 1024) return;
+  static std::mutex mu;
+  static std::map<const void*, size_t> limit;
+  std::lock_guard<std::mutex> lock(mu);
+  size_t& cur = limit[kernel];
+  if (bytes > cur) {
+    VRC_CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    cur = bytes;
+  }
+}
+
 int Engine::gemm_tile_cached(int n, int opA, int opB) const {
   auto it = gemm_tile_.find(n * 4 + opA * 2 + opB);
   return it == gemm_tile_.end() ? 0 : it->second;

@@ -272,8 +272,12 @@ class Engine {
     long long launches = 0;
     double flops = 0.0;  // algorithmic real FP64 flops
     double bytes = 0.0;  // algorithmic bytes moved
+    std::vector<std::pair<double, double>> iv;  // launch intervals (ms after the time origin)
   };
   void set_profiling(bool on);
+  // Event that launch intervals are measured from (one event shared by the
+  // engines of a context, so their intervals share one time line).
+  void set_time_origin(cudaEvent_t e) { origin_ = e; }
   bool profiling() const { return profiling_; }
   std::map<std::string, FamStat>& fam_stats();
   void reset_fam_stats();
@@ -298,6 +302,7 @@ class Engine {
   void* ws_ = nullptr;
   size_t ws_cap_ = 0;
   bool profiling_ = false;
+  cudaEvent_t origin_ = nullptr;
   // host-bubble diagnostic (VRC_HOST_STATS): time from a sync's return to
   // the next profiled launch, when the GPU has nothing queued
  public:

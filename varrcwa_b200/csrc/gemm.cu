@@ -205,16 +205,9 @@ __global__ void __launch_bounds__(TL::THREADS, 512 / TL::THREADS)
 template <class TL>
 void launch_tile(const GemmDesc* d_descs, int batch, int n, cplx alpha, cplx beta, double delta,
                  cudaStream_t stream, int kdim, int opA, int opB) {
-  static bool configured = false;
-  if (!configured) {
-    VRC_CUDA_CHECK(cudaFuncSetAttribute(zgemm_kernel<TL, 0, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, TL::SMEM));
-    VRC_CUDA_CHECK(cudaFuncSetAttribute(zgemm_kernel<TL, 1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, TL::SMEM));
-    VRC_CUDA_CHECK(cudaFuncSetAttribute(zgemm_kernel<TL, 0, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, TL::SMEM));
-    VRC_CUDA_CHECK(cudaFuncSetAttribute(zgemm_kernel<TL, 1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, TL::SMEM));
-    configured = true;
-  }
   auto kern = opA ? (opB ? zgemm_kernel<TL, 1, 1> : zgemm_kernel<TL, 1, 0>)
                   : (opB ? zgemm_kernel<TL, 0, 1> : zgemm_kernel<TL, 0, 0>);
+  ensure_smem((const void*)kern, TL::SMEM);
   const int tiles = ((n + TL::BM - 1) / TL::BM) * ((n + TL::BN - 1) / TL::BN);
   for (int b0 = 0; b0 < batch; b0 += 65535) {
     int nb = batch - b0 < 65535 ? batch - b0 : 65535;

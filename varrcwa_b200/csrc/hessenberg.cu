@@ -441,12 +441,7 @@ bool hessenberg_cluster_fits(int n) { return n >= 3 && n <= HG_MAXN; }
 void hessenberg_cluster_batched(cplx* const* d_H, cplx* const* d_Z, int batch, int n, cudaStream_t st) {
   if (batch <= 0) return;
   if (n > HC_THREADS || hc_layout(n).total > 227 * 1024) {
-    static bool gconf = false;
-    if (!gconf) {
-      VRC_CUDA_CHECK(cudaFuncSetAttribute(hess_cluster_global_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)HG_SMEM));
-      gconf = true;
-    }
+    ensure_smem((const void*)hess_cluster_global_kernel, HG_SMEM);
     for (int b0 = 0; b0 < batch; b0 += 65535) {
       const int nb = min(65535, batch - b0);
       hess_cluster_global_kernel<<<dim3(HC_CS, nb), HC_THREADS, HG_SMEM, st>>>(d_H + b0, d_Z + b0, n);
@@ -455,12 +450,7 @@ void hessenberg_cluster_batched(cplx* const* d_H, cplx* const* d_Z, int batch, i
     return;
   }
   const size_t smem = hc_layout(n).total;
-  static size_t configured = 0;
-  if (smem > configured) {
-    VRC_CUDA_CHECK(
-        cudaFuncSetAttribute(hess_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    configured = smem;
-  }
+  ensure_smem((const void*)hess_cluster_kernel, smem);
   for (int b0 = 0; b0 < batch; b0 += 65535) {
     const int nb = min(65535, batch - b0);
     hess_cluster_kernel<<<dim3(HC_CS, nb), HC_THREADS, smem, st>>>(d_H + b0, d_Z + b0, n);

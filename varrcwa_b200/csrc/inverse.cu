@@ -531,20 +531,11 @@ void zinv_blocked_batched(cplx* const* d_mats, int batch, int n, int* d_status, 
   const int W = zinv_blocked_width(n);
   const size_t per = zinv_blocked_scratch(n) / 16;
   const size_t smem = (size_t)(W + 1) * n * 16 + (size_t)n * 4 + 2 * W * 4;
-  static size_t configured = 0;
-  if (smem > configured && smem > 48 * 1024) {
-    VRC_CUDA_CHECK(cudaFuncSetAttribute(zinv_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    configured = smem;
-  }
+  ensure_smem((const void*)zinv_panel_kernel, smem);
   // registers hold the panel when every row has a thread of each half
   const bool use_reg = n <= 256 && W == 32 && !std::getenv("VRC_ZINV_SMEM_PANEL");
   const size_t reg_smem = RPN_STAGE + (256 + 64) * sizeof(int);
-  static bool reg_configured = false;
-  if (use_reg && !reg_configured) {
-    VRC_CUDA_CHECK(
-        cudaFuncSetAttribute(zinv_panel_reg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)reg_smem));
-    reg_configured = true;
-  }
+  if (use_reg) ensure_smem((const void*)zinv_panel_reg_kernel, reg_smem);
   cplx* scr = static_cast<cplx*>(scratch);
   for (int b0 = 0; b0 < batch; b0 += 65535) {
     const int nb = min(65535, batch - b0);
@@ -570,12 +561,7 @@ void zinv_batched(cplx* const* d_mats, int batch, int n, int* d_status, cudaStre
   if (batch <= 0) return;
   int nb = zinv_panel_width(n);
   size_t smem = (size_t)(nb + 1) * n * 16 + (size_t)n * 4;
-  static int configured_smem = 0;
-  if ((int)smem > configured_smem && smem > 48 * 1024) {
-    VRC_CUDA_CHECK(cudaFuncSetAttribute(zinv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)smem));
-    configured_smem = (int)smem;
-  }
+  ensure_smem((const void*)zinv_kernel, smem);
   for (int b0 = 0; b0 < batch; b0 += 65535) {
     int nbat = batch - b0 < 65535 ? batch - b0 : 65535;
     zinv_kernel<<<nbat, INV_THREADS, smem, stream>>>(d_mats + b0, n, nb,

@@ -6,6 +6,11 @@
 
 namespace vrc {
 
+// Raise a kernel's dynamic shared-memory limit to at least `bytes` (above the
+// 48 KB default).  The limit only grows, under a lock, so launchers may run
+// from several host threads (one engine per thread).
+void ensure_smem(const void* kernel, size_t bytes);
+
 // ---- GEMM: C = diag(rs) (alpha A B) diag(cs) + beta Cin + delta I -----------
 struct GemmDesc {
   const cplx* A;

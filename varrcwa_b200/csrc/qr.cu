@@ -620,15 +620,9 @@ __global__ void __launch_bounds__(RP_THREADS, 4)
 void schur_batched(cplx* const* d_H, cplx* const* d_Z, cplx* const* d_W, void* const* d_logs, int batch, int n,
                    int* d_status, cudaStream_t st, int parts) {
   if (batch <= 0) return;
-  static bool configured = false;
-  if (!configured) {
-    VRC_CUDA_CHECK(cudaFuncSetAttribute(hqr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)QR_SMEM));
-    VRC_CUDA_CHECK(
-        cudaFuncSetAttribute(qr_replay_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RP_SMEM));
-    VRC_CUDA_CHECK(
-        cudaFuncSetAttribute(qr_replay_cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RP_SMEM));
-    configured = true;
-  }
+  ensure_smem((const void*)hqr_kernel, QR_SMEM);
+  ensure_smem((const void*)qr_replay_rows_kernel, RP_SMEM);
+  ensure_smem((const void*)qr_replay_cols_kernel, RP_SMEM);
   const int cc = schur_sweep_cap(n);
   const long long rc = schur_rot_cap(n);
   const int row_blocks = (n + RP_THREADS - 1) / RP_THREADS;
