@@ -17,6 +17,7 @@ struct vrc_context {
   // concurrently, each with its own stream, memory pools and host thread
   std::vector<std::unique_ptr<vrc::Engine>> lanes;
   cudaEvent_t origin = nullptr;  // time origin of the profiled launch intervals
+  int stack_lanes = 1;           // lanes of the last vrc_stack_forward (its tape lives there)
   std::string err;
   vrc_timing timing{0.0, 0};
   std::vector<std::vector<vrc::NodeRecord>> trees;
@@ -177,30 +178,24 @@ int lane_count(int ncells) {
   return std::max(1, std::min({g, 8, std::max(ncells, 1)}));
 }
 
-// Deals the cells round-robin over the lanes and runs
-// solve(lane index, engine, cells, their indices in the call, results) on
-// every lane in its own host thread.  Results come back in call order with
-// the lane that owns each one (its device blocks live in that engine).
-template <class F>
-void run_lanes(vrc_context* ctx, const std::vector<vrc::CellSpec>& specs, std::vector<vrc::CellResult>& res,
-               std::vector<int>& owner, F&& solve) {
-  const int C = (int)specs.size();
-  const int G = lane_count(C);
+void ensure_lanes(vrc_context* ctx, int G) {
   while ((int)ctx->lanes.size() < G - 1) {
     auto e = std::make_unique<vrc::Engine>(ctx->eng->device());
     e->set_profiling(ctx->eng->profiling());
     e->set_time_origin(ctx->origin);
     ctx->lanes.push_back(std::move(e));
   }
-  std::vector<std::vector<vrc::CellSpec>> gs(G);
-  std::vector<std::vector<int>> ids(G);
-  for (int c = 0; c < C; ++c) {
-    gs[c % G].push_back(specs[c]);
-    ids[c % G].push_back(c);
-  }
-  std::vector<std::vector<vrc::CellResult>> out(G);
-  for (int g = 1; g < G; ++g)  // lane work starts after the call's first event
-    VRC_CUDA_CHECK(cudaStreamWaitEvent(lane(ctx, g).stream(), ctx->ev0, 0));
+}
+
+// Runs fn(g, engine of lane g) for g = 0..G-1, lanes 1.. in their own host
+// threads after the call's first event on the context's stream; the
+// context's stream then waits for every lane, so the call's device time spans
+// all of them.  The first exception is rethrown after every lane finished
+// (cleanup(g) runs on every lane first).
+template <class F, class Cleanup>
+void for_lanes(vrc_context* ctx, int G, F&& fn, Cleanup&& cleanup) {
+  ensure_lanes(ctx, G);
+  for (int g = 1; g < G; ++g) VRC_CUDA_CHECK(cudaStreamWaitEvent(lane(ctx, g).stream(), ctx->ev0, 0));
   std::vector<std::exception_ptr> err(G);
   std::vector<std::thread> th;
   const int dev = ctx->eng->device();
@@ -208,13 +203,13 @@ void run_lanes(vrc_context* ctx, const std::vector<vrc::CellSpec>& specs, std::v
     th.emplace_back([&, g] {
       try {
         VRC_CUDA_CHECK(cudaSetDevice(dev));
-        solve(g, lane(ctx, g), gs[g], ids[g], out[g]);
+        fn(g, lane(ctx, g));
       } catch (...) {
         err[g] = std::current_exception();
       }
     });
   try {
-    solve(0, *ctx->eng, gs[0], ids[0], out[0]);
+    fn(0, *ctx->eng);
   } catch (...) {
     err[0] = std::current_exception();
   }
@@ -223,12 +218,10 @@ void run_lanes(vrc_context* ctx, const std::vector<vrc::CellSpec>& specs, std::v
     if (err[g]) {
       for (int h = 0; h < G; ++h) {
         lane(ctx, h).sync();
-        for (auto& r : out[h]) lane(ctx, h).release_result(r);
+        cleanup(h);
       }
       std::rethrow_exception(err[g]);
     }
-  // the context's stream waits for every lane, so the call's device time
-  // spans all of them
   for (int g = 1; g < G; ++g) {
     cudaEvent_t ev;
     VRC_CUDA_CHECK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
@@ -236,6 +229,29 @@ void run_lanes(vrc_context* ctx, const std::vector<vrc::CellSpec>& specs, std::v
     VRC_CUDA_CHECK(cudaStreamWaitEvent(ctx->eng->stream(), ev, 0));
     VRC_CUDA_CHECK(cudaEventDestroy(ev));
   }
+}
+
+// Deals the cells round-robin over the lanes and runs
+// solve(lane index, engine, cells, their indices in the call, results) on
+// every lane.  Results come back in call order with the lane that owns each
+// one (its device blocks live in that engine).
+template <class F>
+void run_lanes(vrc_context* ctx, const std::vector<vrc::CellSpec>& specs, std::vector<vrc::CellResult>& res,
+               std::vector<int>& owner, F&& solve) {
+  const int C = (int)specs.size();
+  const int G = lane_count(C);
+  std::vector<std::vector<vrc::CellSpec>> gs(G);
+  std::vector<std::vector<int>> ids(G);
+  for (int c = 0; c < C; ++c) {
+    gs[c % G].push_back(specs[c]);
+    ids[c % G].push_back(c);
+  }
+  std::vector<std::vector<vrc::CellResult>> out(G);
+  for_lanes(
+      ctx, G, [&](int g, vrc::Engine& E) { solve(g, E, gs[g], ids[g], out[g]); },
+      [&](int g) {
+        for (auto& r : out[g]) lane(ctx, g).release_result(r);
+      });
   res.assign(C, vrc::CellResult());
   owner.assign(C, 0);
   for (int g = 0; g < G; ++g)
@@ -573,7 +589,33 @@ int vrc_stack_forward(vrc_context* ctx, int nstacks, const vrc_stack* stacks, do
       o.eps_out = vrc::mk(s.eps_out.re, s.eps_out.im);
     }
     Timed tm(ctx);
-    ctx->eng->stack_forward(specs, px, py, REF, TRN, status);
+    // stacks dealt round-robin over the lanes; each lane keeps the tape of
+    // its own stacks for vrc_stack_backward
+    const int G = lane_count(nstacks);
+    const int m = specs[0].nx * specs[0].ny;
+    std::vector<std::vector<vrc::Engine::StackSpec>> gs(G);
+    for (int c = 0; c < nstacks; ++c) gs[c % G].push_back(specs[c]);
+    std::vector<std::vector<double>> lr(G), lt(G);
+    std::vector<std::vector<int>> ls(G);
+    ctx->stack_lanes = 1;
+    for (int g = 0; g < (int)ctx->lanes.size() + 1; ++g) lane(ctx, g).release_stack_tape();
+    for_lanes(
+        ctx, G,
+        [&](int g, vrc::Engine& E) {
+          const size_t k = gs[g].size();
+          lr[g].resize(k * m);
+          lt[g].resize(k * m);
+          ls[g].resize(k);
+          E.stack_forward(gs[g], px, py, lr[g].data(), lt[g].data(), ls[g].data());
+        },
+        [&](int g) { lane(ctx, g).release_stack_tape(); });
+    ctx->stack_lanes = G;
+    for (int c = 0; c < nstacks; ++c) {
+      const int g = c % G, k = c / G;
+      std::memcpy(REF + (size_t)c * m, lr[g].data() + (size_t)k * m, m * sizeof(double));
+      std::memcpy(TRN + (size_t)c * m, lt[g].data() + (size_t)k * m, m * sizeof(double));
+      if (status) status[c] = ls[g][k];
+    }
     tm.done();
   });
 }
@@ -581,8 +623,29 @@ int vrc_stack_forward(vrc_context* ctx, int nstacks, const vrc_stack* stacks, do
 int vrc_stack_backward(vrc_context* ctx, const double* wR, const double* wT, double* grad_eps) {
   return guarded(ctx, [&] {
     if (!wR || !wT || !grad_eps) throw vrc::StatusError(VRC_EINVAL, "invalid arguments");
+    const int G = ctx->stack_lanes;
+    const vrc::Engine::StackTape& t0 = ctx->eng->stack_tape();
+    if (t0.C == 0) throw vrc::StatusError(VRC_EINVAL, "stack backward: no forward solve to differentiate");
+    const int m = t0.m;
+    const size_t per = (size_t)t0.L * t0.npx * t0.npy;
+    int nst = 0;
+    for (int g = 0; g < G; ++g) nst += lane(ctx, g).stack_tape().C;
     Timed tm(ctx);
-    ctx->eng->stack_backward(wR, wT, grad_eps);
+    std::vector<std::vector<double>> wr(G), wt(G), gr(G);
+    for (int c = 0; c < nst; ++c) {
+      const int g = c % G;
+      wr[g].insert(wr[g].end(), wR + (size_t)c * m, wR + (size_t)(c + 1) * m);
+      wt[g].insert(wt[g].end(), wT + (size_t)c * m, wT + (size_t)(c + 1) * m);
+    }
+    for_lanes(
+        ctx, G,
+        [&](int g, vrc::Engine& E) {
+          gr[g].resize((size_t)E.stack_tape().C * per);
+          E.stack_backward(wr[g].data(), wt[g].data(), gr[g].data());
+        },
+        [](int) {});
+    for (int c = 0; c < nst; ++c)
+      std::memcpy(grad_eps + (size_t)c * per, gr[c % G].data() + (size_t)(c / G) * per, per * sizeof(double));
     tm.done();
   });
 }

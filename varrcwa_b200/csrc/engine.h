@@ -330,6 +330,7 @@ class Engine {
   struct EndBasis {
     cplx *W, *V, *Winv, *Vinv, *gam;
   };
+ public:
   // Device state of the last stack_forward (one block per stack).
   struct StackLayer {
     cplx *P, *Q, *W, *V, *Winv, *Vinv, *gam, *A, *B, *Ainv, *x, *fe33inv, *eps;
@@ -351,6 +352,9 @@ class Engine {
     std::vector<StackCell> cells;
     std::vector<int> status;
   };
+  const StackTape& stack_tape() const { return tape_; }
+
+ private:
   StackTape tape_;
   std::map<int, int> gemm_tile_;  // key n * 4 + opA * 2 + opB
 };
