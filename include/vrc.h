@@ -198,7 +198,8 @@ int vrc_order_powers(vrc_context* ctx, int ncells, const vrc_cell* cells, int me
  * vrc_stack_forward on the context.
  * vrc_stack_backward returns grad_eps (nstacks * nlayers * npy * npx) =
  * dL/d(eps pixel) for L = sum_k wR[k] REF[k] + wT[k] TRN[k] (wR, wT:
- * nstacks * nx*ny weights each).  The adjoint covers the star-product chain,
+ * nstacks * nx*ny weights each) and, when grad_thick is not NULL,
+ * dL/d(layer thickness) (nstacks * nlayers), a geometric parameter.  The adjoint covers the star-product chain,
  * the eigen step (exact first-order layer perturbation in fixed bases, valid
  * for degenerate eigenvalues) and the Fourier-Toeplitz assembly. */
 typedef struct {
@@ -212,7 +213,7 @@ typedef struct {
 } vrc_stack;
 int vrc_stack_forward(vrc_context* ctx, int nstacks, const vrc_stack* stacks, double px, double py, double* REF,
                       double* TRN, int* status);
-int vrc_stack_backward(vrc_context* ctx, const double* wR, const double* wT, double* grad_eps);
+int vrc_stack_backward(vrc_context* ctx, const double* wR, const double* wT, double* grad_eps, double* grad_thick);
 
 /* ---- instrumentation (no counterpart in the reference) ---------------------
  * Per-kernel-family device time measured with CUDA events on the engine

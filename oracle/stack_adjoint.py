@@ -380,10 +380,12 @@ def assembly_adjoint(st: Stack, eps, gP, gQ):
     return gf.real
 
 
-def stack_backward(st: Stack, tp: Tape, wR, wT, want_pq=False):
+def stack_backward(st: Stack, tp: Tape, wR, wT, want_pq=False, want_thick=False):
     """Gradient of L = sum_k wR[k] REF[k] + wT[k] TRN[k] with respect to every
     pixel of every layer.  Returns a list of (npy, npx) real arrays (and the
-    per-layer (dL/dP, dL/dQ) when want_pq)."""
+    per-layer (dL/dP, dL/dQ) when want_pq, and dL/d(thickness) per layer when
+    want_thick: a layer's own-basis blocks depend on its thickness only
+    through X = diag(exp(i gamma d / k0)), dX/dd = (i gamma / k0) X)."""
     smp = st.sampler()
     k0 = smp.k0
     n = smp.ndim
@@ -392,16 +394,24 @@ def stack_backward(st: Stack, tp: Tape, wR, wT, want_pq=False):
     G = [Zn, gTuu, Zn, gRdu]
     G = project_right_adjoint(tp.Sc, tp.ABr, tp.S, G)
     grads, pq = [None] * len(st.layers), [None] * len(st.layers)
+    gthick = np.zeros(len(st.layers))
     for l in range(len(st.layers) - 1, -1, -1):
         b = tp.bases[l]
         d = st.thick[l]
         X = np.diag(np.exp(1j * b.gam * d / k0))
         G, gseg = star_adjoint(tp.prefix[l], tp.segs[l], G)
         gown = project_left_adjoint([X, X, Zn, Zn], tp.AB[l], tp.segs[l], gseg)
+        dX = (1j * b.gam / k0) * np.diag(X)
+        gthick[l] = float(np.real(np.sum(np.conj(np.diag(gown[0]) + np.diag(gown[1])) * dX)))
         gP, gQ = layer_pq_adjoint(b, d, k0, gown)
         pq[l] = (gP, gQ)
         grads[l] = assembly_adjoint(st, st.layers[l], gP, gQ)
-    return (grads, pq) if want_pq else grads
+    out = [grads]
+    if want_pq:
+        out.append(pq)
+    if want_thick:
+        out.append(gthick)
+    return out[0] if len(out) == 1 else tuple(out)
 
 
 def order_index(nx, ny, ox, oy):

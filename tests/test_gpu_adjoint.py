@@ -139,3 +139,30 @@ def test_stack_lanes_match_one_engine(ctx, monkeypatch):
         out[lanes] = (R, T, st, ctx.stack_backward(wR, wT))
     for a, b in zip(out["1"], out["3"]):
         assert np.array_equal(a, b)
+
+
+def test_thickness_gradient(ctx):
+    """dL/d(layer thickness) against the oracle and against fourth-order
+    central differences solved on the device in one batch."""
+    nx = 3
+    layers = [smooth_pixels(4700 + l, 8, 8, sigma=1.0) for l in range(3)]
+    thick = [0.12, 0.2, 0.15]
+    wR, wT = _weights(nx)
+    ctx.stack_forward([_desc(layers, thick, nx)])
+    _, gt = ctx.stack_backward(wR, wT, want_thick=True)
+    ost, (_, _, tp) = _oracle(_desc(layers, thick, nx))
+    _, ogt = stack_backward(ost, tp, wR[0], wT[0], want_thick=True)
+    assert np.abs(gt[0] - ogt).max() <= 1e-9 * np.abs(ogt).max()
+    h = 1e-4
+    batch = []
+    for l in range(3):
+        for s in (2.0, 1.0, -1.0, -2.0):
+            t2 = list(thick)
+            t2[l] += s * h
+            batch.append(_desc(layers, t2, nx))
+    R, T, st = ctx.stack_forward(batch)
+    assert (st == 0).all()
+    L = (R * wR[0]).sum(axis=1) + (T * wT[0]).sum(axis=1)
+    f = L.reshape(3, 4)
+    fd = (8.0 * (f[:, 1] - f[:, 2]) - (f[:, 0] - f[:, 3])) / (12.0 * h)
+    assert np.abs(fd - gt[0]).max() <= 1e-6 * np.abs(gt).max()

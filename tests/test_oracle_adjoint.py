@@ -80,3 +80,26 @@ def test_smooth_pixels_range(seed):
     p = smooth_pixels(seed, 64, 64)
     assert p.shape == (64, 64) and p.min() >= 2.085 and p.max() <= 12.11
     assert p.max() - p.min() > 5.0
+
+
+def test_thickness_gradient_matches_central_differences():
+    layers = [smooth_pixels(4600 + l, 8, 8, sigma=1.0) for l in range(3)]
+    thick = [0.12, 0.2, 0.15]
+    wR = np.linspace(0.2, 0.0, 9)
+    wT = np.zeros(9)
+    wT[order_index(3, 3, 1, 0)] = 1.0
+    st = _stack(layers, thick)
+    _, _, tp = stack_forward(st)
+    _, gt = stack_backward(st, tp, wR, wT, want_thick=True)
+    # fourth-order central differences: the objective oscillates with the
+    # thickness on the scale k0 / gamma ~ 0.03 um, so a second-order stencil
+    # would need h ~ 1e-6 and meet rounding there
+    h = 1e-4
+    for l in range(3):
+        vals = []
+        for s in (2.0, 1.0, -1.0, -2.0):
+            t2 = list(thick)
+            t2[l] += s * h
+            vals.append(_objective(_stack(layers, t2), wR, wT))
+        fd = (8.0 * (vals[1] - vals[2]) - (vals[0] - vals[3])) / (12.0 * h)
+        assert abs(fd - gt[l]) <= 1e-7 * np.abs(gt).max(), (l, fd, gt[l])

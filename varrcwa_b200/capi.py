@@ -124,7 +124,7 @@ def lib():
     DP = C.POINTER(C.c_double)
     L.vrc_stack_forward.argtypes = [vp, C.c_int, C.POINTER(VrcStack), C.c_double, C.c_double, DP, DP,
                                     C.POINTER(C.c_int)]
-    L.vrc_stack_backward.argtypes = [vp, DP, DP, DP]
+    L.vrc_stack_backward.argtypes = [vp, DP, DP, DP, DP]
     _lib = L
     return L
 
@@ -429,12 +429,14 @@ class Context:
         self._stack_shape = (len(stacks), len(stacks[0]["layers"]), *np.asarray(stacks[0]["layers"][0]).shape)
         return REF, TRN, st
 
-    def stack_backward(self, wR: np.ndarray, wT: np.ndarray):
-        """dL/d(pixel) of L = sum wR*REF + wT*TRN for the last stack_forward;
-        shape (nstacks, nlayers, npy, npx)."""
+    def stack_backward(self, wR: np.ndarray, wT: np.ndarray, want_thick: bool = False):
+        """dL/d(pixel) of L = sum wR*REF + wT*TRN for the last stack_forward,
+        shape (nstacks, nlayers, npy, npx); with want_thick also dL/d(layer
+        thickness), shape (nstacks, nlayers)."""
         shape = self._stack_shape
         wR = np.ascontiguousarray(np.broadcast_to(np.asarray(wR, dtype=np.float64), (shape[0], wR.shape[-1])))
         wT = np.ascontiguousarray(np.broadcast_to(np.asarray(wT, dtype=np.float64), (shape[0], wT.shape[-1])))
         g = np.zeros(shape)
-        self._check(self.L.vrc_stack_backward(self.h, _dptr(wR), _dptr(wT), _dptr(g)))
-        return g
+        gt = np.zeros(shape[:2])
+        self._check(self.L.vrc_stack_backward(self.h, _dptr(wR), _dptr(wT), _dptr(g), _dptr(gt)))
+        return (g, gt) if want_thick else g

@@ -104,6 +104,28 @@ __global__ void layer_adjoint_kernel(const LayerAdjDesc* __restrict__ ds, int n)
   }
 }
 
+// The thickness enters a layer's own-basis blocks only through
+// X = diag(exp(i gam d / k0)); dX/dd = (i gam / k0) X.
+__global__ void thick_adjoint_kernel(const ThickAdjDesc* __restrict__ ds, int n) {
+  const ThickAdjDesc d = ds[blockIdx.x];
+  __shared__ double red[32];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const size_t ii = (size_t)i * n + i;
+    const cplx g = cadd(d.gtdd[ii], d.gtuu[ii]);
+    const cplx dx = cmul(mk(-d.gam[i].y / d.k0, d.gam[i].x / d.k0), d.x[i]);  // (i gam / k0) x
+    s += g.x * dx.x + g.y * dx.y;                                              // Re(conj(g) dx)
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    *d.out = t;
+  }
+}
+
 // dL/dP, dL/dQ of Layer::waveEqnCoeff (src/rcwa/Layer.cpp:36-171, periodic)
 // -> dL/dfe11, dL/dfe22 and Z = dL/dF1 Kx + dL/dF2 Ky (F = fe33^-1 [Kx Ky]).
 __global__ void pq_adjoint_kernel(const PQAdjDesc* __restrict__ ds, int m) {
@@ -516,6 +538,12 @@ void layer_adjoint_batched(const LayerAdjDesc* d, int batch, int n, cudaStream_t
 void pq_adjoint_batched(const PQAdjDesc* d, int batch, int m, cudaStream_t st) {
   if (batch <= 0) return;
   pq_adjoint_kernel<<<grid_for((long long)m * m, batch), 256, 0, st>>>(d, m);
+  VRC_CUDA_CHECK(cudaGetLastError());
+}
+
+void thick_adjoint_batched(const ThickAdjDesc* d, int batch, int n, cudaStream_t st) {
+  if (batch <= 0) return;
+  thick_adjoint_kernel<<<batch, 256, 0, st>>>(d, n);
   VRC_CUDA_CHECK(cudaGetLastError());
 }
 

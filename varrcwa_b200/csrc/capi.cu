@@ -620,7 +620,7 @@ int vrc_stack_forward(vrc_context* ctx, int nstacks, const vrc_stack* stacks, do
   });
 }
 
-int vrc_stack_backward(vrc_context* ctx, const double* wR, const double* wT, double* grad_eps) {
+int vrc_stack_backward(vrc_context* ctx, const double* wR, const double* wT, double* grad_eps, double* grad_thick) {
   return guarded(ctx, [&] {
     if (!wR || !wT || !grad_eps) throw vrc::StatusError(VRC_EINVAL, "invalid arguments");
     const int G = ctx->stack_lanes;
@@ -631,7 +631,7 @@ int vrc_stack_backward(vrc_context* ctx, const double* wR, const double* wT, dou
     int nst = 0;
     for (int g = 0; g < G; ++g) nst += lane(ctx, g).stack_tape().C;
     Timed tm(ctx);
-    std::vector<std::vector<double>> wr(G), wt(G), gr(G);
+    std::vector<std::vector<double>> wr(G), wt(G), gr(G), gth(G);
     for (int c = 0; c < nst; ++c) {
       const int g = c % G;
       wr[g].insert(wr[g].end(), wR + (size_t)c * m, wR + (size_t)(c + 1) * m);
@@ -641,11 +641,16 @@ int vrc_stack_backward(vrc_context* ctx, const double* wR, const double* wT, dou
         ctx, G,
         [&](int g, vrc::Engine& E) {
           gr[g].resize((size_t)E.stack_tape().C * per);
-          E.stack_backward(wr[g].data(), wt[g].data(), gr[g].data());
+          gth[g].resize((size_t)E.stack_tape().C * t0.L);
+          E.stack_backward(wr[g].data(), wt[g].data(), gr[g].data(), gth[g].data());
         },
         [](int) {});
-    for (int c = 0; c < nst; ++c)
+    for (int c = 0; c < nst; ++c) {
       std::memcpy(grad_eps + (size_t)c * per, gr[c % G].data() + (size_t)(c / G) * per, per * sizeof(double));
+      if (grad_thick)
+        std::memcpy(grad_thick + (size_t)c * t0.L, gth[c % G].data() + (size_t)(c / G) * t0.L,
+                    t0.L * sizeof(double));
+    }
     tm.done();
   });
 }

@@ -259,7 +259,8 @@ class Engine {
                      int* status);
   // Gradient of L = sum_k wR[k] REF[k] + wT[k] TRN[k] (m weights each per
   // stack) with respect to every pixel of every layer (L * npy * npx per stack).
-  void stack_backward(const double* wR, const double* wT, double* grad);
+  // grad_thick (L per stack, may be null): dL/d(layer thickness).
+  void stack_backward(const double* wR, const double* wT, double* grad, double* grad_thick = nullptr);
   void release_stack_tape();
 
   // counters

@@ -143,6 +143,14 @@ struct PixAdjDesc {
   double* grad;                    // npy x npx
   double Lx, Ly;
 };
+// dL/d(thickness) of a layer: Re sum_i conj(gtdd_ii + gtuu_ii) (i gam_i / k0) x_i
+// with x = exp(i gam d / k0) (one CTA per layer).
+struct ThickAdjDesc {
+  const cplx *gtdd, *gtuu, *gam, *x;
+  double* out;
+  double k0;
+};
+void thick_adjoint_batched(const ThickAdjDesc* d, int batch, int n, cudaStream_t st);
 bool pixel_adjoint_fits(int nx, int ny, int npx, int npy);
 void pixel_adjoint_batched(const PixAdjDesc* d, int batch, int nx, int ny, int npx, int npy, cudaStream_t st);
 struct StackPowerDesc {

@@ -323,7 +323,7 @@ void Engine::stack_forward(const std::vector<StackSpec>& stacks, double px, doub
   if (status) std::memcpy(status, tp.status.data(), C * sizeof(int));
 }
 
-void Engine::stack_backward(const double* wR, const double* wT, double* grad) {
+void Engine::stack_backward(const double* wR, const double* wT, double* grad, double* grad_thick) {
   StackTape& tp = tape_;
   if (tp.C == 0) throw StatusError(ST_EINVAL, "stack backward: no forward solve to differentiate");
   const int C = tp.C, L = tp.L, n = tp.n, m = tp.m, npx = tp.npx, npy = tp.npy;
@@ -374,6 +374,7 @@ void Engine::stack_backward(const double* wR, const double* wT, double* grad) {
   bt.release(gTuu_n, n);
   bt.release(gRdu_n, n);
   double* dgrad = (double*)bytes((size_t)C * L * npx * npy * 8);
+  double* dthick = (double*)bytes((size_t)C * L * 8);
   Vec GP[4];
   for (auto& g : GP) g = bt.alloc(n);
   Vec gs[4];
@@ -449,6 +450,14 @@ void Engine::stack_backward(const double* wR, const double* wT, double* grad) {
     bt.mm(o_rdu, Y, A, ONE, 0, 1, nullptr, ZERO, n);
     bt.mm(o_rdu, T4, B, MONE, 0, 1, &o_rdu, ONE, n);                   // grdu = gY A^H - gM B^H
     // grud of the own-basis blocks is grud' itself (gs[2])
+    {
+      std::vector<ThickAdjDesc> td(C);
+      for (int c = 0; c < C; ++c)
+        td[c] = {o_tdd[c], o_tuu[c], tp.cells[c].lay[l].gam, tp.cells[c].lay[l].x, dthick + (size_t)c * L + l,
+                 2.0 * 3.1415926535897932 / tp.specs[c].lambda};
+      Prof pr(*this, "adjoint", 0.0, 32.0 * n * (double)C);
+      thick_adjoint_batched(upload(td), C, n, stream_);
+    }
     // ---- exact first-order layer kernel -> dL/dP, dL/dQ ----
     {
       std::vector<LayerAdjDesc> ld(C);
@@ -490,11 +499,14 @@ void Engine::stack_backward(const double* wR, const double* wT, double* grad) {
     }
     for (int k = 0; k < 4; ++k) std::swap(G[k], GP[k]);
   }
-  std::vector<double> hg((size_t)C * L * npx * npy);
+  std::vector<double> hg((size_t)C * L * npx * npy), ht((size_t)C * L);
   VRC_CUDA_CHECK(cudaMemcpyAsync(hg.data(), dgrad, hg.size() * 8, cudaMemcpyDeviceToHost, stream_));
+  VRC_CUDA_CHECK(cudaMemcpyAsync(ht.data(), dthick, ht.size() * 8, cudaMemcpyDeviceToHost, stream_));
   sync();
   std::memcpy(grad, hg.data(), hg.size() * 8);
+  if (grad_thick) std::memcpy(grad_thick, ht.data(), ht.size() * 8);
   free_bytes(dgrad, (size_t)C * L * npx * npy * 8);
+  free_bytes(dthick, (size_t)C * L * 8);
   free_bytes(dw, (size_t)2 * C * m * 8);
   free_bytes(dR, (size_t)2 * C * m * 8);
   for (Vec* v : {&T1, &T2, &T3, &T4, &C1, &C1r, &C2, &X1, &X2, &Y, &Zm, &RC1, &U, &gC1, &gC2}) bt.release(*v, n);
