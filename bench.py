@@ -57,6 +57,7 @@ def parse():
     p.add_argument("--plain-cells", type=int, default=8,
                    help="cells timed one per call (the plain per-solve form of the metric); 0 skips")
     p.add_argument("--no-adjoint", action="store_true", help="skip the fwd_adjoint sub-measurement of the c2 line")
+    p.add_argument("--orders", type=int, default=9, help="c4: harmonics per axis (9 = config 4, 15 = 15x15 orders)")
     a = p.parse_args()
     if a.pe is None:
         a.pe = 1e-6 if a.workload == "c1" else 1e-2
@@ -65,9 +66,9 @@ def parse():
     return a
 
 
-def make_cells(workload, batch, rank, npix, step_seed=0):
+def make_cells(workload, batch, rank, npix, step_seed=0, orders=9):
     from varrcwa_b200.replicas import make_cells as mc
-    return mc(workload, batch, rank, npix, step_seed)
+    return mc(workload, batch, rank, npix, step_seed, orders)
 
 
 # ---------------------------------------------------------------------------
@@ -202,7 +203,7 @@ def run_reference(a, rank, world):
         return  # rank 0 alone times the CPU reference
     ncores = os.cpu_count() or 1
     workers = max(1, ncores)
-    descs = make_cells(a.workload, workers, rank, a.npix)
+    descs = make_cells(a.workload, workers, rank, a.npix, orders=a.orders)
     os.environ["OPENBLAS_NUM_THREADS"] = "1"
     os.environ["OMP_NUM_THREADS"] = "1"
     os.environ["MKL_NUM_THREADS"] = "1"
@@ -270,8 +271,10 @@ def unit_name(workload="c2"):
 
 def workload_config(a, batch):
     if a.workload == "c4":
-        return {"workload": "config-4 freeform metagrating stacks (9x9 orders, n=162, 4 layers x 64x64 pixels, "
-                            "600 nm period, 633 nm, air -> SiO2)", "batch_per_gpu": batch, "n": 162,
+        o = a.orders
+        return {"workload": f"config-4 freeform metagrating stacks ({o}x{o} orders, n={2 * o * o}, 4 layers x "
+                            f"64x64 pixels, 600 nm period, 633 nm, air -> SiO2)", "batch_per_gpu": batch,
+                "n": 2 * o * o,
                 "integrator": "Redheffer chain of z-uniform layers (one eigen-solve per layer), star products",
                 "output": "per-order R/T (x-polarised incidence) and dT(+1,0)/d(eps) for all 16384 pixels",
                 "l2": "per-step working set (GBs of matrices) exceeds the 126 MB L2; no flush needed"}
@@ -299,9 +302,9 @@ def run_ours(a, rank, world, local_rank):
     dev = local_rank
     torch.cuda.set_device(dev)
     ctx = Context(dev)
-    descs = make_cells(a.workload, a.batch, rank, a.npix)
+    descs = make_cells(a.workload, a.batch, rank, a.npix, orders=a.orders)
 
-    solve = make_solver(ctx, a.workload, a.pe, a.batch)
+    solve = make_solver(ctx, a.workload, a.pe, a.batch, a.orders)
 
     def barrier():
         if world > 1:
@@ -447,12 +450,12 @@ def roofline_of(stats, fp64_peak):
     return roof
 
 
-def make_solver(ctx, workload, pe, batch):
+def make_solver(ctx, workload, pe, batch, orders=9):
     """One step of the workload through the C ABI: returns (per-cell results,
     device ms, kernel launches) of the call(s)."""
     import numpy as np
     if workload == "c4":
-        nx = ny = 9
+        nx = ny = orders
         k = ny * (1 + (nx - 1) // 2) + (ny - 1) // 2  # order (+1, 0)
         wT = np.zeros((batch, nx * ny))
         wT[:, k] = 1.0

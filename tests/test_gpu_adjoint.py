@@ -166,3 +166,21 @@ def test_thickness_gradient(ctx):
     f = L.reshape(3, 4)
     fd = (8.0 * (f[:, 1] - f[:, 2]) - (f[:, 0] - f[:, 3])) / (12.0 * h)
     assert np.abs(fd - gt[0]).max() <= 1e-6 * np.abs(gt).max()
+
+
+def test_fifteen_orders_stack_matches_oracle(ctx):
+    """15 x 15 orders (n = 450): the pixel adjoint keeps its Toeplitz-diagonal
+    sums in global scratch and runs with fewer warps per CTA."""
+    nx = 15
+    layers = [smooth_pixels(4800 + l, 16, 16, sigma=1.5) for l in range(2)]
+    d = _desc(layers, [0.15, 0.1], nx)
+    R, T, st = ctx.stack_forward([d])
+    assert st[0] == 0
+    ost, (oR, oT, tp) = _oracle(d)
+    assert np.abs(R[0] - oR).max() < 1e-9 and np.abs(T[0] - oT).max() < 1e-9
+    m = nx * nx
+    wT = np.zeros((1, m))
+    wT[0, order_index(nx, nx, 1, 0)] = 1.0
+    g = ctx.stack_backward(np.zeros((1, m)), wT)[0]
+    og = np.array(stack_backward(ost, tp, np.zeros(m), wT[0]))
+    assert np.abs(g - og).max() <= 1e-8 * np.abs(og).max()

@@ -222,33 +222,38 @@ __host__ __device__ inline int px_warp_scratch(int t) { return 3 * t * t + 2 * (
 // uniform npy x npx grid (FourierSolver2D::solve, src/rcwa/FourierSolver2D.cpp:
 // 43-349: Laurent rule for fe33, Li's inverse rule for fe11 (y strips) and
 // fe22 (x columns)).  The per-strip Toeplitz inverses are recomputed here.
+// The Toeplitz-diagonal sums of dL/dfe11 and dL/dfe22 (K11, K22: read by every
+// strip) go to a global scratch of the layer (L2 resident), so that 15 x 15
+// orders fit; the CTA has as many warps as its shared memory allows.
 __global__ void __launch_bounds__(PX_THREADS)
     pixel_adjoint_kernel(const PixAdjDesc* __restrict__ ds, int nx, int ny, int npx, int npy) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const PixAdjDesc d = ds[blockIdx.x];
   const int P = 2 * nx - 1, Q = 2 * ny - 1, m = nx * ny, t = nx > ny ? nx : ny;
+  const int NW = blockDim.x >> 5;
   cplx* Ex = reinterpret_cast<cplx*>(smem_raw);  // [npx][P]
   cplx* Ey = Ex + (size_t)P * npx;               // [npy][Q]
-  cplx* K11 = Ey + (size_t)Q * npy;              // [Q][nx][nx]
-  cplx* K22 = K11 + (size_t)Q * nx * nx;         // [P][ny][ny]
-  cplx* gf = K22 + (size_t)P * ny * ny;          // [Q][P]
+  cplx* gf = Ey + (size_t)Q * npy;               // [Q][P]
   cplx* H1 = gf + (size_t)P * Q;                 // [Q][npx]
   cplx* wsc = H1 + (size_t)Q * npx;              // per-warp scratch
-  double* acc = reinterpret_cast<double*>(wsc + (size_t)PX_WARPS * px_warp_scratch(t));  // [npy][npx]
+  double* acc = reinterpret_cast<double*>(wsc + (size_t)NW * px_warp_scratch(t));  // [npy][npx]
   int* pivs = reinterpret_cast<int*>(acc + (size_t)npy * npx);
+  cplx* K11 = d.kscr;                            // [Q][nx][nx]
+  cplx* K22 = d.kscr + (size_t)Q * nx * nx;      // [P][ny][ny]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int NT = blockDim.x;
 
-  for (int idx = tid; idx < P * npx; idx += PX_THREADS) {
+  for (int idx = tid; idx < P * npx; idx += NT) {
     const int c = idx / P, p = idx - c * P;
     Ex[idx] = twiddle(p, nx - 1, d.Lx * c / npx, d.Lx * (c + 1) / npx, d.Lx);
   }
-  for (int idx = tid; idx < Q * npy; idx += PX_THREADS) {
+  for (int idx = tid; idx < Q * npy; idx += NT) {
     const int r = idx / Q, q = idx - r * Q;
     Ey[idx] = twiddle(q, ny - 1, d.Ly * r / npy, d.Ly * (r + 1) / npy, d.Ly);
   }
   auto G = [&](const cplx* M, int a, int c, int b, int dd) { return M[(size_t)(b * ny + dd) * m + a * ny + c]; };
   // Toeplitz-diagonal sums of the three Fourier-block adjoints
-  for (int idx = tid; idx < Q * nx * nx; idx += PX_THREADS) {
+  for (int idx = tid; idx < Q * nx * nx; idx += NT) {
     const int q = idx / (nx * nx), rem = idx - q * nx * nx, b = rem / nx, a = rem - b * nx;
     const int qq = q - (ny - 1);
     cplx s = mk(0.0, 0.0);
@@ -258,7 +263,7 @@ __global__ void __launch_bounds__(PX_THREADS)
     }
     K11[idx] = s;
   }
-  for (int idx = tid; idx < P * ny * ny; idx += PX_THREADS) {
+  for (int idx = tid; idx < P * ny * ny; idx += NT) {
     const int p = idx / (ny * ny), rem = idx - p * ny * ny, dd = rem / ny, c = rem - dd * ny;
     const int pp = p - (nx - 1);
     cplx s = mk(0.0, 0.0);
@@ -268,7 +273,7 @@ __global__ void __launch_bounds__(PX_THREADS)
     }
     K22[idx] = s;
   }
-  for (int idx = tid; idx < P * Q; idx += PX_THREADS) {
+  for (int idx = tid; idx < P * Q; idx += NT) {
     const int q = idx / P, p = idx - q * P;
     const int pp = p - (nx - 1), qq = q - (ny - 1);
     cplx s = mk(0.0, 0.0);
@@ -284,14 +289,14 @@ __global__ void __launch_bounds__(PX_THREADS)
   }
   __syncthreads();
   // fe33 (Laurent rule): four = Ex f^T Ey^T  ->  df = Ey^H-weighted sums
-  for (int idx = tid; idx < Q * npx; idx += PX_THREADS) {
+  for (int idx = tid; idx < Q * npx; idx += NT) {
     const int q = idx / npx, c = idx - q * npx;
     cplx s = mk(0.0, 0.0);
     for (int p = 0; p < P; ++p) s = cadd(s, cmulc(Ex[c * P + p], gf[q * P + p]));
     H1[idx] = s;
   }
   __syncthreads();
-  for (int idx = tid; idx < npy * npx; idx += PX_THREADS) {
+  for (int idx = tid; idx < npy * npx; idx += NT) {
     const int r = idx / npx, c = idx - r * npx;
     double s = 0.0;
     for (int q = 0; q < Q; ++q) {
@@ -309,7 +314,7 @@ __global__ void __launch_bounds__(PX_THREADS)
   cplx* fcol = gv + (2 * t - 1);   // t
   int* piv = pivs + warp * 32;
   // fe11: one y strip r per warp pass; T_r = inv(Toep(Ex (1/eps[r, :])))
-  for (int r = warp; r < npy; r += PX_WARPS) {
+  for (int r = warp; r < npy; r += NW) {
     const cplx* er = d.eps + (size_t)r * npx;
     for (int p = lane; p < P; p += 32) {
       cplx s = mk(0.0, 0.0);
@@ -368,7 +373,7 @@ __global__ void __launch_bounds__(PX_THREADS)
   }
   __syncthreads();
   // fe22: one x column i per warp pass; T_i = inv(Toep(Ey (1/eps[:, i])))
-  for (int i = warp; i < npx; i += PX_WARPS) {
+  for (int i = warp; i < npx; i += NW) {
     for (int q = lane; q < Q; q += 32) {
       cplx s = mk(0.0, 0.0);
       for (int r = 0; r < npy; ++r) s = cadd(s, cmul(Ey[r * Q + q], cinv(d.eps[(size_t)r * npx + i])));
@@ -422,7 +427,7 @@ __global__ void __launch_bounds__(PX_THREADS)
     __syncwarp();
   }
   __syncthreads();
-  for (int idx = tid; idx < npy * npx; idx += PX_THREADS) d.grad[idx] = acc[idx];
+  for (int idx = tid; idx < npy * npx; idx += NT) d.grad[idx] = acc[idx];
 }
 
 // Per-order powers of a stack (RCWASolver::scatterPlaneWave,
@@ -547,24 +552,33 @@ void thick_adjoint_batched(const ThickAdjDesc* d, int batch, int n, cudaStream_t
   VRC_CUDA_CHECK(cudaGetLastError());
 }
 
-size_t pixel_adjoint_smem(int nx, int ny, int npx, int npy) {
+size_t pixel_adjoint_smem(int nx, int ny, int npx, int npy, int nw) {
   const int P = 2 * nx - 1, Q = 2 * ny - 1, t = nx > ny ? nx : ny;
-  size_t c = (size_t)P * npx + (size_t)Q * npy + (size_t)Q * nx * nx + (size_t)P * ny * ny + (size_t)P * Q +
-             (size_t)Q * npx + (size_t)PX_WARPS * px_warp_scratch(t);
-  return c * 16 + (size_t)npy * npx * 8 + PX_WARPS * 32 * sizeof(int);
+  size_t c = (size_t)P * npx + (size_t)Q * npy + (size_t)P * Q + (size_t)Q * npx + (size_t)nw * px_warp_scratch(t);
+  return c * 16 + (size_t)npy * npx * 8 + (size_t)nw * 32 * sizeof(int);
 }
 
-bool pixel_adjoint_fits(int nx, int ny, int npx, int npy) {
-  return nx <= 32 && ny <= 32 && pixel_adjoint_smem(nx, ny, npx, npy) <= 227 * 1024;
+// warps per CTA: the most (up to eight) whose shared memory fits; 0 if none
+int pixel_adjoint_warps(int nx, int ny, int npx, int npy) {
+  if (nx > 32 || ny > 32) return 0;
+  for (int nw = PX_WARPS; nw >= 1; nw /= 2)
+    if (pixel_adjoint_smem(nx, ny, npx, npy, nw) <= 227 * 1024) return nw;
+  return 0;
+}
+
+bool pixel_adjoint_fits(int nx, int ny, int npx, int npy) { return pixel_adjoint_warps(nx, ny, npx, npy) > 0; }
+
+size_t pixel_adjoint_scratch(int nx, int ny) {
+  return ((size_t)(2 * ny - 1) * nx * nx + (size_t)(2 * nx - 1) * ny * ny) * 16;
 }
 
 void pixel_adjoint_batched(const PixAdjDesc* d, int batch, int nx, int ny, int npx, int npy, cudaStream_t st) {
   if (batch <= 0) return;
-  if (!pixel_adjoint_fits(nx, ny, npx, npy))
-    throw StatusError(ST_EINVAL, "pixel adjoint: raster and harmonics exceed the shared-memory tile");
-  const size_t smem = pixel_adjoint_smem(nx, ny, npx, npy);
+  const int nw = pixel_adjoint_warps(nx, ny, npx, npy);
+  if (!nw) throw StatusError(ST_EINVAL, "pixel adjoint: raster and harmonics exceed the shared-memory tile");
+  const size_t smem = pixel_adjoint_smem(nx, ny, npx, npy, nw);
   ensure_smem((const void*)pixel_adjoint_kernel, smem);
-  pixel_adjoint_kernel<<<batch, PX_THREADS, smem, st>>>(d, nx, ny, npx, npy);
+  pixel_adjoint_kernel<<<batch, nw * 32, smem, st>>>(d, nx, ny, npx, npy);
   VRC_CUDA_CHECK(cudaGetLastError());
 }
 

@@ -141,6 +141,7 @@ struct PixAdjDesc {
   const cplx* eps;                 // npy x npx, row-major (rows = y strips)
   const cplx *g11, *g22, *g33;     // m x m
   double* grad;                    // npy x npx
+  cplx* kscr;                      // pixel_adjoint_scratch(nx, ny) bytes of device scratch
   double Lx, Ly;
 };
 // dL/d(thickness) of a layer: Re sum_i conj(gtdd_ii + gtuu_ii) (i gam_i / k0) x_i
@@ -152,6 +153,7 @@ struct ThickAdjDesc {
 };
 void thick_adjoint_batched(const ThickAdjDesc* d, int batch, int n, cudaStream_t st);
 bool pixel_adjoint_fits(int nx, int ny, int npx, int npy);
+size_t pixel_adjoint_scratch(int nx, int ny);
 void pixel_adjoint_batched(const PixAdjDesc* d, int batch, int nx, int ny, int npx, int npy, cudaStream_t st);
 struct StackPowerDesc {
   const cplx *W0, *W0inv, *W1, *Tuu, *Rdu;

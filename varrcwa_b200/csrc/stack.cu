@@ -375,6 +375,8 @@ void Engine::stack_backward(const double* wR, const double* wT, double* grad, do
   bt.release(gRdu_n, n);
   double* dgrad = (double*)bytes((size_t)C * L * npx * npy * 8);
   double* dthick = (double*)bytes((size_t)C * L * 8);
+  const size_t kper = pixel_adjoint_scratch(tp.nx, tp.ny);
+  char* kscr = (char*)bytes((size_t)C * kper);
   Vec GP[4];
   for (auto& g : GP) g = bt.alloc(n);
   Vec gs[4];
@@ -492,8 +494,8 @@ void Engine::stack_backward(const double* wR, const double* wT, double* grad, do
     {
       std::vector<PixAdjDesc> xd(C);
       for (int c = 0; c < C; ++c)
-        xd[c] = {tp.cells[c].lay[l].eps, g11[c], g22[c], g33[c],
-                 dgrad + ((size_t)c * L + l) * npx * npy, tp.specs[c].Lx, tp.specs[c].Ly};
+        xd[c] = {tp.cells[c].lay[l].eps, g11[c], g22[c], g33[c], dgrad + ((size_t)c * L + l) * npx * npy,
+                 reinterpret_cast<cplx*>(kscr + (size_t)c * kper), tp.specs[c].Lx, tp.specs[c].Ly};
       Prof pr(*this, "adjoint", 0.0, 16.0 * (3.0 * m * m + (double)npx * npy) * C);
       pixel_adjoint_batched(upload(xd), C, tp.nx, tp.ny, npx, npy, stream_);
     }
@@ -507,6 +509,7 @@ void Engine::stack_backward(const double* wR, const double* wT, double* grad, do
   if (grad_thick) std::memcpy(grad_thick, ht.data(), ht.size() * 8);
   free_bytes(dgrad, (size_t)C * L * npx * npy * 8);
   free_bytes(dthick, (size_t)C * L * 8);
+  free_bytes(kscr, (size_t)C * kper);
   free_bytes(dw, (size_t)2 * C * m * 8);
   free_bytes(dR, (size_t)2 * C * m * 8);
   for (Vec* v : {&T1, &T2, &T3, &T4, &C1, &C1r, &C2, &X1, &X2, &Y, &Zm, &RC1, &U, &gC1, &gC2}) bt.release(*v, n);

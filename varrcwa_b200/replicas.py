@@ -22,7 +22,7 @@ def cell_seeds(workload: str, batch: int, rank: int, step_seed: int = 0) -> List
     return [base + i for i in range(batch)]
 
 
-def make_cells(workload: str, batch: int, rank: int, npix: int, step_seed: int = 0):
+def make_cells(workload: str, batch: int, rank: int, npix: int, step_seed: int = 0, orders: int = 9):
     import numpy as np
 
     from . import structures as st
@@ -32,7 +32,7 @@ def make_cells(workload: str, batch: int, rank: int, npix: int, step_seed: int =
     if workload == "c2":
         return [st.pillar_config2(seed=s, npix=npix) for s in seeds]
     if workload == "c4":  # freeform metagrating stacks (npix is the 256 raster of c2/c3; c4 keeps 64x64)
-        return [st.metagrating_c4(seed=s) for s in seeds]
+        return [st.metagrating_c4(seed=s, norders=orders) for s in seeds]
     return [st.pillar_config3(seed=s, npix=npix) for s in seeds]
 
 

@@ -170,13 +170,14 @@ def smooth_pixels(seed, npx, npy, sigma=3.0, beta=8.0, lo=2.085, hi=12.11):
     return lo + (hi - lo) * t
 
 
-def metagrating_c4(seed=4000, npix=64, nlayers=4):
+def metagrating_c4(seed=4000, npix=64, nlayers=4, norders=9):
     """Freeform metagrating of config 4: 600 nm square period, 633 nm, 9x9
-    orders (n = 162), four 150 nm layers of npix x npix pixels (smoothed
+    orders (n = 162; norders sets another truncation, e.g. 15 for the
+    15x15-order comparison), four 150 nm layers of npix x npix pixels (smoothed
     thresholded noise in [2.085, 12.11], layer l seeded by (seed, l)).
     Incidence from air below; transmission into the SiO2 substrate (eps
     2.085), where the (+1, 0) order propagates (it is evanescent in air at
     this period)."""
     layers = [smooth_pixels([seed, l], npix, npix) for l in range(nlayers)]
-    return dict(lam=0.633, Lx=0.6, Ly=0.6, nx=9, ny=9, layers=layers, thick=[0.15] * nlayers,
+    return dict(lam=0.633, Lx=0.6, Ly=0.6, nx=norders, ny=norders, layers=layers, thick=[0.15] * nlayers,
                 eps_in=1.0, eps_out=2.085)
