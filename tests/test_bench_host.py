@@ -47,3 +47,21 @@ def test_profiled_traffic_scales_by_matrices(bench):
     assert per_launch_one is not None and per_launch_one > 0
     assert bench.profiled_traffic("schur_qr", 2 * 40 * 242 ** 3) == pytest.approx(2 * per_launch_one)
     assert bench.profiled_traffic("no_such_family", 1.0) is None
+
+
+def test_roofline_uses_union_time_and_launched_families(bench):
+    """The dominant family is chosen among launched kernels (host_alloc is
+    host time) by its busy time, the union of its launch intervals, which
+    is also the denominator of the achieved rate."""
+    stats = {
+        "host_alloc": {"ms": 9000.0, "busy_ms": 9000.0, "launches": 0, "flops": 0.0, "bytes": 0.0},
+        "schur_qr": {"ms": 3000.0, "busy_ms": 1000.0, "launches": 6, "flops": 4.0e12, "bytes": 0.0},
+        "zgemm": {"ms": 900.0, "busy_ms": 800.0, "launches": 100, "flops": 2.4e13, "bytes": 0.0},
+        "assembly": {"ms": 100.0, "busy_ms": 90.0, "launches": 50, "flops": 0.0, "bytes": 1e9},
+    }
+    r = bench.roofline_of(stats, 35.0)
+    assert r["kernel"] == "schur_qr" and r["bound"] == "tensor"
+    assert r["achieved"] == pytest.approx(4.0)           # 4e12 flops over 1.0 s busy
+    assert r["frac"] == pytest.approx(4.0 / 35.0)
+    assert r["avg_launch_ms"] == pytest.approx(500.0)    # summed durations per launch
+    assert r["busy_ms"] == 1000.0
