@@ -35,6 +35,7 @@ struct Batch {
   int C;
   void mm(const Vec& Cm, const Vec& A, const Vec& B, cplx alpha = ONE, int oa = 0, int ob = 0,
           const Vec* Cin = nullptr, cplx beta = ZERO, int n = 0, const Vec* rs = nullptr, double delta = 0.0) {
+    if (n <= 0) throw StatusError(ST_EINVAL, "stack GEMM without an order");
     std::vector<GemmDesc> d(C);
     for (int c = 0; c < C; ++c)
       d[c] = {A[c], B[c], Cm[c], Cin ? (*Cin)[c] : nullptr, rs ? (*rs)[c] : nullptr, nullptr};
