@@ -45,7 +45,8 @@ enum vrc_status_code {
 enum vrc_geometry_kind {
   VRC_GEOM_GRID = 0,   /* tensor grid, fixed eps table, moving coordinates */
   VRC_GEOM_PILLAR = 1, /* uniform raster of a circular pillar, linear radius */
-  VRC_GEOM_PIXELS = 2  /* fixed uniform pixel raster (z-invariant) */
+  VRC_GEOM_PIXELS = 2, /* fixed uniform pixel raster (z-invariant) */
+  VRC_GEOM_PLANAR = 3  /* planar device seen from above: layout polygons in (x, z) */
 };
 
 /* Piecewise-linear z-rule for one coordinate (clamped outside [zs0, zsN]).
@@ -93,6 +94,21 @@ typedef struct {
    * eigen-bases there, as the reference integrators do) */
   int has_end0, has_end1;
   vrc_complex eps_end0, eps_end1;
+  /* VRC_GEOM_PLANAR: replaces GDSIISampler(lambda, nx, ny, filename, shift,
+   * lPML, rPML, lspace, rspace, bPML, uPML, bspace, uspace, permBackground,
+   * permDevice, thickness) (src/core/GDSIISampler.h:25-35).  Polygons lie in
+   * the layout plane (x across, z along the propagation); at every z the
+   * cross-section is the device layer (thickness along y) cut by the
+   * polygons, between spacers and PML on all four sides (pml is ignored:
+   * always on).  vrc_gds_read loads the polygons of a GDSII file. */
+  int npoly;
+  const int* poly_start;  /* npoly + 1 point offsets into poly_xz */
+  const double* poly_xz;  /* (x, z) pairs */
+  double shift[3];        /* x, y, z */
+  double pml_w[4];        /* left, right, bottom, top PML widths */
+  double space[4];        /* left, right, bottom, top spaces between PML and device */
+  double thickness;
+  vrc_complex eps_background, eps_device;
 } vrc_cell;
 
 /* Outputs of one integration.  Matrix pointers may be NULL (not copied). */
@@ -214,6 +230,21 @@ typedef struct {
 int vrc_stack_forward(vrc_context* ctx, int nstacks, const vrc_stack* stacks, double px, double py, double* REF,
                       double* TRN, int* status);
 int vrc_stack_backward(vrc_context* ctx, const double* wR, const double* wT, double* grad_eps, double* grad_thick);
+
+/* ---- GDSII layouts ---------------------------------------------------------
+ * BOUNDARY and BOX polygons of the first structure of a GDSII file (the
+ * polygons gdstk::read_gds gives GDSIISampler, src/core/GDSIISampler.cpp:32),
+ * coordinates in units of `unit` metres (1e-6: micrometres).  Sets npoly and
+ * npoints; fills poly_start (npoly + 1 offsets) and poly_xz (2 * npoints)
+ * when both are given and large enough (else VRC_EINVAL).  No context and
+ * no GPU needed. */
+int vrc_gds_read(const char* path, double unit, int* npoly, int* npoints, int* poly_start, double* poly_xz,
+                 int max_poly, int max_points);
+/* Cross-section of a VRC_GEOM_PLANAR cell at z (GDSIISampler::sampleLayout,
+ * src/core/GDSIISampler.cpp:90-140): x (returned count, at most max_x), the
+ * six y coordinates and the 5 x (count - 1) eps table (rows are y strips).
+ * With NULL outputs only the count is returned; negative on error. */
+int vrc_planar_section(const vrc_cell* cell, double z, int max_x, double* x, double* y, vrc_complex* eps);
 
 /* ---- instrumentation (no counterpart in the reference) ---------------------
  * Per-kernel-family device time measured with CUDA events on the engine

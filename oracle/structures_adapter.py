@@ -48,6 +48,11 @@ def make_sampler(d):
         eps = np.asarray(d["eps"], dtype=np.complex128)
         return O.RasterSampler(d["lam"], d["nx"], d["ny"], d["Lx"], d["Ly"],
                                lambda z: eps, enable_pml=d["pml"])
+    if kind == "planar":
+        from .planar_sampler import PlanarSampler
+        return PlanarSampler(d["lam"], d["nx"], d["ny"], d["polys"], d.get("shift", (0.0, 0.0, 0.0)),
+                             d.get("pml_w", (0.5, 0.5, 0.5, 0.5)), d.get("space", (1.5, 1.5, 1.08, 1.0)),
+                             d.get("thickness", 0.22), d["eps_bg"], d["eps_dev"])
     raise ValueError(kind)
 
 

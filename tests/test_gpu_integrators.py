@@ -130,3 +130,27 @@ def test_lanes_match_one_engine(ctx, monkeypatch):
             assert np.array_equal(a[k], b[k])
         assert a["N"] == b["N"]
     assert out["1"][2] == out["3"][2]
+
+
+def test_planar_gds_cell_matches_oracle(ctx):
+    """A planar (GDS-style) taper seen from above: per-z cross-sections with
+    a varying number of x cells, PML on all four sides.  P, Q against the
+    oracle's GDSIISampler restatement, then adaptive varRCWA against the
+    oracle replayed on the device's tree."""
+    from oracle.structures_adapter import make_sampler
+    from varrcwa_b200 import structures as st
+    d = st.planar_taper(norders=(7, 3))
+    zs = [0.3, 0.5, 1.7, 2.9, 4.5, 4.6]
+    P, Q = ctx.sample_pq(d, zs)
+    s = make_sampler(d)
+    for k, z in enumerate(zs):
+        oP, oQ = s.sample(z)
+        assert relerr(P[k], oP) < 1e-12 and relerr(Q[k], oQ) < 1e-12, z
+    r = ctx.redheffer([d], pe=1e-2)[0]
+    assert r["status"] == 0 and r["N"] >= 1
+    leaves = sorted((a, b) for (a, b, e, acc) in ctx.tree(0) if acc)
+    cuts = [leaves[0][0]] + [b for (_, b) in leaves]
+    S = O.redheffer_segments(s, d["z0"], d["z1"], cuts)
+    F, G = fourier_blocks(r), S.fourier_blocks()
+    for k in F:
+        assert relerr(F[k], G[k]) < TOL, k

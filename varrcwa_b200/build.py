@@ -20,7 +20,7 @@ BUILD = ROOT / "_build"
 LIB = PKG / "libvrc.so"
 
 SOURCES = ["gemm.cu", "inverse.cu", "eig.cu", "hessenberg.cu", "qr.cu", "assembly.cu", "segment.cu", "engine.cu", "drivers.cu",
-           "capi.cu", "noalloc.cu", "adjoint.cu", "stack.cu"]
+           "capi.cu", "noalloc.cu", "adjoint.cu", "stack.cu", "gds.cu"]
 HEADERS = ["common.cuh", "kernels.h", "engine.h", "householder.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",

@@ -16,14 +16,15 @@ LIB_PATH = Path(__file__).resolve().parent / "libvrc.so"
 
 VRC_OK, VRC_EINVAL, VRC_ECUDA, VRC_ENOMEM, VRC_ESINGULAR, VRC_ENOCONV, VRC_ENONFINITE, VRC_ETIMEOUT, \
     VRC_EDEPTH, VRC_ENODEV = range(10)
-GEOM_GRID, GEOM_PILLAR, GEOM_PIXELS = 0, 1, 2
+GEOM_GRID, GEOM_PILLAR, GEOM_PIXELS, GEOM_PLANAR = 0, 1, 2, 3
 
 # Every function declared in include/vrc.h.
 EXPORTS = [
     "vrc_create", "vrc_destroy", "vrc_last_error", "vrc_status_string", "vrc_get_timing", "vrc_sample_pq",
     "vrc_wave_solve", "vrc_eig", "vrc_redheffer", "vrc_redheffer_segments", "vrc_get_tree", "vrc_rcwa",
     "vrc_differential", "vrc_order_powers", "vrc_zgemm", "vrc_zinv", "vrc_set_profiling",
-    "vrc_get_kernel_stats", "vrc_eig_noalloc", "vrc_stack_forward", "vrc_stack_backward",
+    "vrc_get_kernel_stats", "vrc_eig_noalloc", "vrc_stack_forward", "vrc_stack_backward", "vrc_gds_read",
+    "vrc_planar_section",
 ]
 
 
@@ -51,6 +52,9 @@ class VrcCell(C.Structure):
         ("Lx", C.c_double), ("Ly", C.c_double), ("npx", C.c_int), ("npy", C.c_int),
         ("eps_in", VrcComplex), ("eps_out", VrcComplex), ("r0", C.c_double), ("r1", C.c_double),
         ("has_end0", C.c_int), ("has_end1", C.c_int), ("eps_end0", VrcComplex), ("eps_end1", VrcComplex),
+        ("npoly", C.c_int), ("poly_start", C.POINTER(C.c_int)), ("poly_xz", C.POINTER(C.c_double)),
+        ("shift", C.c_double * 3), ("pml_w", C.c_double * 4), ("space", C.c_double * 4), ("thickness", C.c_double),
+        ("eps_background", VrcComplex), ("eps_device", VrcComplex),
     ]
 
 
@@ -125,6 +129,9 @@ def lib():
     L.vrc_stack_forward.argtypes = [vp, C.c_int, C.POINTER(VrcStack), C.c_double, C.c_double, DP, DP,
                                     C.POINTER(C.c_int)]
     L.vrc_stack_backward.argtypes = [vp, DP, DP, DP, DP]
+    IP = C.POINTER(C.c_int)
+    L.vrc_gds_read.argtypes = [C.c_char_p, C.c_double, IP, IP, IP, DP, C.c_int, C.c_int]
+    L.vrc_planar_section.argtypes = [C.POINTER(VrcCell), C.c_double, C.c_int, DP, DP, CP]
     _lib = L
     return L
 
@@ -149,7 +156,7 @@ class _CellPack:
     def __init__(self, d: dict):
         self.keep = []
         c = VrcCell()
-        kind = {"grid": GEOM_GRID, "pillar": GEOM_PILLAR, "pixels": GEOM_PIXELS}[d["kind"]]
+        kind = {"grid": GEOM_GRID, "pillar": GEOM_PILLAR, "pixels": GEOM_PIXELS, "planar": GEOM_PLANAR}[d["kind"]]
         c.kind = kind
         c.nx, c.ny = int(d["nx"]), int(d["ny"])
         c.pml = 1 if d.get("pml") else 0
@@ -160,6 +167,20 @@ class _CellPack:
             c.npx, c.npy = int(d["npx"]), int(d["npy"])
             c.eps_in, c.eps_out = _vc(d["eps_in"]), _vc(d["eps_out"])
             c.r0, c.r1 = float(d["r0"]), float(d["r1"])
+        elif kind == GEOM_PLANAR:
+            polys = [np.ascontiguousarray(p, dtype=np.float64).reshape(-1, 2) for p in d["polys"]]
+            start = np.ascontiguousarray(np.cumsum([0] + [len(p) for p in polys]), dtype=np.int32)
+            xz = np.ascontiguousarray(np.concatenate(polys).reshape(-1))
+            self.keep += [start, xz]
+            c.npoly = len(polys)
+            c.poly_start = start.ctypes.data_as(C.POINTER(C.c_int))
+            c.poly_xz = _dptr(xz)
+            for name, default in (("shift", (0.0, 0.0, 0.0)), ("pml_w", (0.5, 0.5, 0.5, 0.5)),
+                                  ("space", (1.5, 1.5, 1.08, 1.0))):
+                for q, v in enumerate(d.get(name, default)):
+                    getattr(c, name)[q] = float(v)
+            c.thickness = float(d.get("thickness", 0.22))
+            c.eps_background, c.eps_device = _vc(d["eps_bg"]), _vc(d["eps_dev"])
         else:
             eps = np.ascontiguousarray(d["eps"], dtype=np.complex128)
             if kind == GEOM_PIXELS:
@@ -200,6 +221,39 @@ class _CellPack:
         if d.get("end1") is not None:
             c.has_end1, c.eps_end1 = 1, _vc(d["end1"])
         self.cell = c
+
+
+def gds_read(path, unit: float = 1e-6) -> List[np.ndarray]:
+    """BOUNDARY / BOX polygons of the first structure of a GDSII file, each an
+    (npoints, 2) array of (x, y) in units of `unit` metres (the C reader)."""
+    L = lib()
+    npoly, npts = C.c_int(0), C.c_int(0)
+    st = L.vrc_gds_read(str(path).encode(), float(unit), C.byref(npoly), C.byref(npts), None, None, 0, 0)
+    if st != 0:
+        raise VrcError(st, L.vrc_status_string(st).decode())
+    start = np.zeros(npoly.value + 1, dtype=np.int32)
+    xz = np.zeros(2 * max(npts.value, 1))
+    st = L.vrc_gds_read(str(path).encode(), float(unit), C.byref(npoly), C.byref(npts),
+                        start.ctypes.data_as(C.POINTER(C.c_int)), _dptr(xz), npoly.value, npts.value)
+    if st != 0:
+        raise VrcError(st, L.vrc_status_string(st).decode())
+    return [xz[2 * start[p]:2 * start[p + 1]].reshape(-1, 2).copy() for p in range(npoly.value)]
+
+
+def planar_section(desc: dict, z: float):
+    """Cross-section of a planar cell at z: (x, y, eps (5, len(x) - 1))."""
+    L = lib()
+    pack = _CellPack(desc)
+    n = L.vrc_planar_section(C.byref(pack.cell), float(z), 0, None, None, None)
+    if n < 0:
+        raise VrcError(-n, L.vrc_status_string(-n).decode())
+    x = np.zeros(n)
+    y = np.zeros(6)
+    eps = np.zeros((5, n - 1), dtype=np.complex128)
+    n2 = L.vrc_planar_section(C.byref(pack.cell), float(z), n, _dptr(x), _dptr(y), eps.ctypes.data_as(CP))
+    if n2 != n:
+        raise VrcError(1, "planar section size changed")
+    return x, y, eps
 
 
 class Context:

@@ -144,6 +144,22 @@ vrc::CellSpec to_spec(const vrc_cell& c) {
       void* user = c.geometry_user;
       s.geom_cb = [fn, user](double z, double* x, double* y) { fn(user, z, x, y); };
     }
+  } else if (c.kind == VRC_GEOM_PLANAR) {
+    if (c.npoly < 1 || !c.poly_start || !c.poly_xz) throw vrc::StatusError(VRC_EINVAL, "planar cell needs polygons");
+    s.pml = true;  // GDSIISampler always encloses the device in PML
+    for (int p = 0; p < c.npoly; ++p) {
+      const int a = c.poly_start[p], b = c.poly_start[p + 1];
+      if (a < 0 || b - a < 3) throw vrc::StatusError(VRC_EINVAL, "planar polygons need >= 3 points");
+      s.polys.emplace_back(c.poly_xz + 2 * (size_t)a, c.poly_xz + 2 * (size_t)b);
+    }
+    for (int q = 0; q < 3; ++q) s.shift[q] = c.shift[q];
+    for (int q = 0; q < 4; ++q) {
+      s.pml_w[q] = c.pml_w[q];
+      s.space[q] = c.space[q];
+    }
+    s.thickness = c.thickness;
+    s.eps_bg = vrc::mk(c.eps_background.re, c.eps_background.im);
+    s.eps_dev = vrc::mk(c.eps_device.re, c.eps_device.im);
   } else {
     throw vrc::StatusError(VRC_EINVAL, "unknown geometry kind");
   }
@@ -653,6 +669,55 @@ int vrc_stack_backward(vrc_context* ctx, const double* wR, const double* wT, dou
     }
     tm.done();
   });
+}
+
+int vrc_gds_read(const char* path, double unit, int* npoly, int* npoints, int* poly_start, double* poly_xz,
+                 int max_poly, int max_points) {
+  if (!path || !npoly || !npoints || !(unit > 0.0)) return VRC_EINVAL;
+  try {
+    double dbu = 0.0;
+    auto polys = vrc::gds_read_polygons(path, unit, &dbu);
+    int tot = 0;
+    for (auto& p : polys) tot += (int)(p.size() / 2);
+    *npoly = (int)polys.size();
+    *npoints = tot;
+    if (!poly_start && !poly_xz) return VRC_OK;
+    if (!poly_start || !poly_xz || max_poly < *npoly || max_points < tot) return VRC_EINVAL;
+    int off = 0;
+    for (size_t p = 0; p < polys.size(); ++p) {
+      poly_start[p] = off;
+      std::memcpy(poly_xz + 2 * (size_t)off, polys[p].data(), polys[p].size() * sizeof(double));
+      off += (int)(polys[p].size() / 2);
+    }
+    poly_start[polys.size()] = off;
+    return VRC_OK;
+  } catch (const vrc::StatusError& e) {
+    return e.status;
+  } catch (...) {
+    return VRC_EINVAL;
+  }
+}
+
+int vrc_planar_section(const vrc_cell* cell, double z, int max_x, double* x, double* y, vrc_complex* eps) {
+  if (!cell || cell->kind != VRC_GEOM_PLANAR) return -VRC_EINVAL;
+  try {
+    vrc::CellSpec s = to_spec(*cell);
+    std::vector<double> xs, ys;
+    std::vector<cplx> es;
+    s.planar_section(z, xs, ys, &es);
+    const int nxs = (int)xs.size();
+    if (x && y && eps) {
+      if (max_x < nxs) return -VRC_EINVAL;
+      std::memcpy(x, xs.data(), nxs * sizeof(double));
+      std::memcpy(y, ys.data(), ys.size() * sizeof(double));
+      for (size_t i = 0; i < es.size(); ++i) eps[i] = {es[i].x, es[i].y};
+    }
+    return nxs;
+  } catch (const vrc::StatusError& e) {
+    return -e.status;
+  } catch (...) {
+    return -VRC_EINVAL;
+  }
 }
 
 int vrc_set_profiling(vrc_context* ctx, int enable) {

@@ -142,6 +142,13 @@ void validate(const CellSpec& c) {
   if (!(c.lambda > 0.0)) throw StatusError(ST_EINVAL, "wavelength must be positive");
   if (c.kind == GEOM_PILLAR) {
     if (c.npx < 1 || c.npy < 1) throw StatusError(ST_EINVAL, "pillar raster must be non-empty");
+  } else if (c.kind == GEOM_PLANAR) {
+    if (c.polys.empty()) throw StatusError(ST_EINVAL, "planar cell needs polygons");
+    for (const auto& p : c.polys)
+      if (p.size() < 6 || p.size() % 2) throw StatusError(ST_EINVAL, "planar polygons need >= 3 points");
+    if (!(c.thickness > 0.0)) throw StatusError(ST_EINVAL, "planar device thickness must be positive");
+    for (int q = 0; q < 4; ++q)
+      if (!(c.pml_w[q] > 0.0) || !(c.space[q] >= 0.0)) throw StatusError(ST_EINVAL, "planar PML / spaces invalid");
   } else {
     if (c.x.size() < 2 || c.y.size() < 2) throw StatusError(ST_EINVAL, "grid needs at least 2 coordinates per axis");
     if (c.eps.size() != (c.x.size() - 1) * (c.y.size() - 1))

@@ -34,6 +34,10 @@ double PwlRule::eval(double z) const {
 }
 
 void CellSpec::geometry(double z, std::vector<double>& xo, std::vector<double>& yo) const {
+  if (kind == GEOM_PLANAR) {
+    planar_section(z, xo, yo, nullptr);
+    return;
+  }
   if (kind == GEOM_PILLAR) {
     xo.resize(npx + 1);
     yo.resize(npy + 1);
@@ -532,7 +536,7 @@ Engine::CellDev* Engine::prepare_cell(const CellSpec& c) {
                                {cd->Ky, cd->Kx, cd->KyKx, nullptr, nullptr, nullptr}};
     gemm(g, m, mk(1, 0), mk(0, 0), 0.0);
   }
-  if (c.kind != GEOM_PILLAR) {
+  if (c.kind != GEOM_PILLAR && c.kind != GEOM_PLANAR) {  // planar tables are formed per sample
     cd->eps_count = c.eps.size();
     cd->eps_dev = (cplx*)bytes(cd->eps_count * 16);
     VRC_CUDA_CHECK(cudaMemcpyAsync(cd->eps_dev, c.eps.data(), cd->eps_count * 16, cudaMemcpyHostToDevice, stream_));
@@ -579,6 +583,12 @@ void Engine::assemble(std::vector<SampleReq>& reqs, std::vector<int>* status) {
     if (r.homogeneous) {
       k.ncx = 2;
       k.ncy = 2;
+      k.pillar = 0;
+    } else if (r.spec->kind == GEOM_PLANAR) {  // the cross-section's size depends on z
+      std::vector<double> xs, ys;
+      r.spec->planar_section(r.z, xs, ys, nullptr);
+      k.ncx = (int)xs.size();
+      k.ncy = (int)ys.size();
       k.pillar = 0;
     } else {
       k.ncx = r.spec->ncx();
@@ -663,6 +673,11 @@ void Engine::assemble(std::vector<SampleReq>& reqs, std::vector<int>* status) {
             radius[b] = s.radius(r.z);
             epsw[b] = base + o_eps;
             epsp[b] = base + o_eps;
+          } else if (s.kind == GEOM_PLANAR) {  // crossings come sorted: no refill
+            std::vector<double> px, py;
+            refilled.emplace_back();
+            s.planar_section(r.z, px, py, &refilled.back());
+            epsp[b] = upload(refilled.back());
           } else if (need) {
             refilled.emplace_back(s.eps);
             std::vector<cplx>& nf = refilled.back();

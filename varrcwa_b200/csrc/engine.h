@@ -13,7 +13,7 @@
 
 namespace vrc {
 
-enum GeomKind { GEOM_GRID = 0, GEOM_PILLAR = 1, GEOM_PIXELS = 2 };
+enum GeomKind { GEOM_GRID = 0, GEOM_PILLAR = 1, GEOM_PIXELS = 2, GEOM_PLANAR = 3 };
 
 struct PwlRule {
   int index;
@@ -41,6 +41,19 @@ struct CellSpec {
   // homogeneous end media (otherwise the structure's own bases at z0/z1)
   bool has_end0 = false, has_end1 = false;
   cplx eps_end0{1.0, 0.0}, eps_end1{1.0, 0.0};
+  // planar device seen from above (a GDS layout: x across, z along the
+  // propagation), a device layer of fixed thickness along y, PML all round
+  std::vector<std::vector<double>> polys;  // per polygon x0, z0, x1, z1, ...
+  double shift[3] = {0.0, 0.0, 0.0};       // x, y, z
+  double pml_w[4] = {0.5, 0.5, 0.5, 0.5};  // left, right, bottom, top
+  double space[4] = {1.5, 1.5, 1.08, 1.0};
+  double thickness = 0.22;
+  cplx eps_bg{1.0, 0.0}, eps_dev{1.0, 0.0};
+  // x limits (l0, l1, r0, r1) and the six y coordinates of the planar cell
+  void planar_region(double* xlim, double* y6) const;
+  // cross-section at z: x (crossings between the PML / spacer coordinates),
+  // y, and optionally the (5 x (nx-1)) eps table, rows = y strips
+  void planar_section(double z, std::vector<double>& x, std::vector<double>& y, std::vector<cplx>* eps) const;
 
   int ncx() const { return kind == GEOM_PILLAR ? npx + 1 : (int)x.size(); }
   int ncy() const { return kind == GEOM_PILLAR ? npy + 1 : (int)y.size(); }
@@ -50,6 +63,11 @@ struct CellSpec {
   void geometry(double z, std::vector<double>& xo, std::vector<double>& yo) const;
   double radius(double z) const;
 };
+
+// BOUNDARY and BOX polygons of a GDSII file's first structure, coordinates
+// in `unit` metres (x0, y0, x1, y1, ...); db_unit_m receives the file's
+// metres per database unit.
+std::vector<std::vector<double>> gds_read_polygons(const std::string& path, double unit, double* db_unit_m);
 
 struct NodeRecord {
   double a, b, err;

@@ -181,3 +181,17 @@ def metagrating_c4(seed=4000, npix=64, nlayers=4, norders=9):
     layers = [smooth_pixels([seed, l], npix, npix) for l in range(nlayers)]
     return dict(lam=0.633, Lx=0.6, Ly=0.6, nx=norders, ny=norders, layers=layers, thick=[0.15] * nlayers,
                 eps_in=1.0, eps_out=2.085)
+
+
+def planar_taper(w0=0.5, w1=1.2, length=4.0, lam=1.55, norders=(11, 5), thickness=0.22, eps_bg=EPS_SIO2_BENCH,
+                 eps_dev=EPS_SI_BENCH, lead=0.5):
+    """Planar (GDS-style) silicon taper seen from above: a straight lead of
+    width w0, a linear taper to w1 over `length`, a straight lead of width w1
+    (one polygon in the layout's (x, z) plane), in the device layer of the
+    given thickness; integration over the taper (GDSIISampler's geometry)."""
+    z0, z1 = lead, lead + length
+    pts = [(-0.5 * w0, 0.0), (0.5 * w0, 0.0), (0.5 * w0, z0), (0.5 * w1, z1), (0.5 * w1, z1 + lead),
+           (-0.5 * w1, z1 + lead), (-0.5 * w1, z1), (-0.5 * w0, z0)]
+    return dict(kind="planar", lam=lam, nx=norders[0], ny=norders[1], pml=True, polys=[np.array(pts)],
+                shift=(0.0, 0.0, 0.0), pml_w=(0.5, 0.5, 0.5, 0.5), space=(1.0, 1.0, 0.8, 0.8),
+                thickness=thickness, eps_bg=eps_bg, eps_dev=eps_dev, z0=z0, z1=z1, end0=None, end1=None)
