@@ -231,6 +231,18 @@ int vrc_stack_forward(vrc_context* ctx, int nstacks, const vrc_stack* stacks, do
                       double* TRN, int* status);
 int vrc_stack_backward(vrc_context* ctx, const double* wR, const double* wT, double* grad_eps, double* grad_thick);
 
+/* Internal amplitudes and fields of the stacks of the last vrc_stack_forward
+ * (the role of RCWASolver::evaluateIntermediateField and of its field images,
+ * src/rcwa/RCWASolver.cpp:1373-1480; written to host buffers here).
+ * Interface j = 0..nlayers is the top of region j-1 (region -1: eps_in,
+ * region nlayers: eps_out); amps holds, per stack and interface, the up- then
+ * the down-going mode amplitudes in that region's eigenbasis
+ * (nstacks * (nlayers+1) * 2 * n; j = 0: incident and reflected, j = nlayers:
+ * transmitted and zero).  fields (nstacks * (nlayers+1) * 2 * ngy * ngx, Ex
+ * then Ey, rows of constant y) samples the transverse E field on an
+ * ngx x ngy grid over the period; ngx = ngy = 0 skips it (fields may be NULL). */
+int vrc_stack_fields(vrc_context* ctx, int ngx, int ngy, vrc_complex* amps, vrc_complex* fields);
+
 /* ---- GDSII layouts ---------------------------------------------------------
  * BOUNDARY and BOX polygons of the first structure of a GDSII file (the
  * polygons gdstk::read_gds gives GDSIISampler, src/core/GDSIISampler.cpp:32),

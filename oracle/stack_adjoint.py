@@ -417,3 +417,65 @@ def stack_backward(st: Stack, tp: Tape, wR, wT, want_pq=False, want_thick=False)
 def order_index(nx, ny, ox, oy):
     """Index of diffraction order (ox, oy) in the per-order power vectors."""
     return ny * (ox + (nx - 1) // 2) + (oy + (ny - 1) // 2)
+
+
+# ---------------------------------------------------------------------------
+# Internal amplitudes and fields (the role of RCWASolver::
+# evaluateIntermediateField, src/rcwa/RCWASolver.cpp:1373-1480)
+# ---------------------------------------------------------------------------
+def stack_fields(st: Stack, tp: Tape, ngx=0, ngy=0):
+    """Up- and down-going amplitudes at every interface j = 0..L of the
+    stack for the forward's incidence, and the transverse fields there.
+
+    Interface j is the top of region j-1 (region -1: the entrance medium,
+    region L: the exit medium); amplitudes are in that region's eigenbasis
+    (j = 0: entrance medium, incident c and reflected; j = L: exit medium,
+    transmitted and nothing incoming).  For 0 < j < L, with S_L the chain of
+    layers 0..j-1 and S_R the rest (layers j..L-1 and the exit) whose left
+    end is in the basis of layer j-1:
+        a+ = (I - Rud_L Rdu_R)^-1 Tuu_L c,   a- = Rdu_R a+.
+    Transverse harmonics: e = W (a+ + a-), h = V (a+ - a-) (E and H of the
+    interface matching of RedhefferIntegrator.cpp:253-262).  Returns
+    (amps (L+1, 2, n), e (L+1, n), h (L+1, n), fields (L+1, 2, ngy, ngx) of
+    Ex, Ey on the period when ngx, ngy > 0)."""
+    L = len(st.layers)
+    n = tp.S[0].shape[0]
+    m = n // 2
+    I = np.eye(n, dtype=np.complex128)
+    Z = np.zeros((n, n), np.complex128)
+    c = tp.c
+    last = tp.bases[-1]
+    # exit interface as a zero-thickness S-matrix: left end in the last
+    # layer's basis, right end in the exit medium's
+    SR = project_right([I.copy(), I.copy(), Z.copy(), Z.copy()], last.W, last.V, tp.e1.W, tp.e1.V)
+    suffix = [None] * (L + 1)
+    suffix[L] = SR
+    for j in range(L - 1, 0, -1):
+        suffix[j] = star_right(tp.segs[j], suffix[j + 1])
+    amps = np.zeros((L + 1, 2, n), np.complex128)
+    bases_W = [tp.e0.W] + [b.W for b in tp.bases[:-1]] + [tp.e1.W]
+    bases_V = [tp.e0.V] + [b.V for b in tp.bases[:-1]] + [tp.e1.V]
+    amps[0, 0] = c
+    amps[0, 1] = tp.S[3] @ c
+    for j in range(1, L):
+        SL = tp.prefix[j]
+        SRj = suffix[j]
+        ap = np.linalg.solve(I - SL[2] @ SRj[3], SL[1] @ c)
+        amps[j, 0] = ap
+        amps[j, 1] = SRj[3] @ ap
+    amps[L, 0] = tp.S[1] @ c
+    e = np.array([bases_W[j] @ (amps[j, 0] + amps[j, 1]) for j in range(L + 1)])
+    h = np.array([bases_V[j] @ (amps[j, 0] - amps[j, 1]) for j in range(L + 1)])
+    fields = None
+    if ngx > 0 and ngy > 0:
+        smp = st.sampler()
+        alpha = np.diag(smp.Kx).real
+        beta = np.diag(smp.Ky).real
+        xs = st.Lx * np.arange(ngx) / ngx
+        ys = st.Ly * np.arange(ngy) / ngy
+        ph = np.exp(1j * (alpha[:, None, None] * xs[None, None, :] + beta[:, None, None] * ys[None, :, None]))
+        fields = np.zeros((L + 1, 2, ngy, ngx), np.complex128)
+        for j in range(L + 1):
+            fields[j, 0] = np.tensordot(e[j, :m], ph, axes=(0, 0))
+            fields[j, 1] = np.tensordot(e[j, m:], ph, axes=(0, 0))
+    return amps, e, h, fields

@@ -184,3 +184,23 @@ def test_fifteen_orders_stack_matches_oracle(ctx):
     g = ctx.stack_backward(np.zeros((1, m)), wT)[0]
     og = np.array(stack_backward(ost, tp, np.zeros(m), wT[0]))
     assert np.abs(g - og).max() <= 1e-8 * np.abs(og).max()
+
+
+@pytest.mark.parametrize("lanes", ["1", "3"])
+def test_internal_fields_match_oracle(ctx, monkeypatch, lanes):
+    """Transverse E images at every interface (basis invariant) against the
+    oracle, for stacks solved on one and on three lanes."""
+    from oracle.stack_adjoint import stack_fields
+    monkeypatch.setenv("VRC_LANES", lanes)
+    nx = 3
+    ds = [_desc([smooth_pixels([5100, i, l], 8, 8, sigma=1.0) for l in range(3)], [0.15, 0.1 + 0.02 * i, 0.2], nx)
+          for i in range(6)]
+    ctx.stack_forward(ds)
+    amps, img = ctx.stack_fields(8, 6)
+    assert amps.shape == (6, 4, 2, 18) and img.shape == (6, 4, 2, 6, 8)
+    for i, d in enumerate(ds):
+        ost, (_, oT, tp) = _oracle(d)
+        _, _, _, of = stack_fields(ost, tp, 8, 6)
+        assert np.abs(img[i] - of).max() <= 1e-9 * np.abs(of).max()
+        # entrance: the incident amplitudes are c = W0^-1 s, the exit has nothing incoming
+        assert np.abs(amps[i, -1, 1]).max() == 0.0

@@ -103,3 +103,22 @@ def test_thickness_gradient_matches_central_differences():
             vals.append(_objective(_stack(layers, t2), wR, wT))
         fd = (8.0 * (vals[1] - vals[2]) - (vals[0] - vals[3])) / (12.0 * h)
         assert abs(fd - gt[l]) <= 1e-7 * np.abs(gt).max(), (l, fd, gt[l])
+
+
+def test_internal_fields_conserve_flux():
+    """The amplitudes at every interface carry the same z-power flux,
+    Re sum(ex conj(hy) - ey conj(hx)) over the harmonics, equal to the
+    transmitted power (lossless stack), and the field images are the
+    harmonic sums on the period grid."""
+    from oracle.stack_adjoint import stack_fields
+    layers = [smooth_pixels([5000, l], 8, 8, sigma=1.0) for l in range(3)]
+    st = Stack(LAM, 3, 3, PER, PER, layers, [0.15, 0.1, 0.2], eps_in=1.0, eps_out=2.085)
+    R, T, tp = stack_forward(st)
+    amps, e, h, f = stack_fields(st, tp, 6, 5)
+    m = 9
+    flux = [np.real(np.vdot(h[j, m:], e[j, :m]) - np.vdot(h[j, :m], e[j, m:])) for j in range(4)]
+    assert np.ptp(flux) < 1e-12 and abs(flux[0] - T.sum()) < 1e-12 and abs(1 - R.sum() - flux[0]) < 1e-12
+    assert f.shape == (4, 2, 5, 6)
+    # the centre pixel-free check: the mean of Ex over the period is the zero harmonic
+    k0 = (3 * (3 - 1)) // 2 + (3 - 1) // 2
+    np.testing.assert_allclose(f[:, 0].mean(axis=(1, 2)), e[:, k0], rtol=0, atol=1e-13)

@@ -24,7 +24,7 @@ EXPORTS = [
     "vrc_wave_solve", "vrc_eig", "vrc_redheffer", "vrc_redheffer_segments", "vrc_get_tree", "vrc_rcwa",
     "vrc_differential", "vrc_order_powers", "vrc_zgemm", "vrc_zinv", "vrc_set_profiling",
     "vrc_get_kernel_stats", "vrc_eig_noalloc", "vrc_stack_forward", "vrc_stack_backward", "vrc_gds_read",
-    "vrc_planar_section",
+    "vrc_planar_section", "vrc_stack_fields",
 ]
 
 
@@ -130,6 +130,7 @@ def lib():
                                     C.POINTER(C.c_int)]
     L.vrc_stack_backward.argtypes = [vp, DP, DP, DP, DP]
     IP = C.POINTER(C.c_int)
+    L.vrc_stack_fields.argtypes = [vp, C.c_int, C.c_int, CP, CP]
     L.vrc_gds_read.argtypes = [C.c_char_p, C.c_double, IP, IP, IP, DP, C.c_int, C.c_int]
     L.vrc_planar_section.argtypes = [C.POINTER(VrcCell), C.c_double, C.c_int, DP, DP, CP]
     _lib = L
@@ -481,6 +482,7 @@ class Context:
         self._check(self.L.vrc_stack_forward(self.h, len(stacks), arr, float(px), float(py), _dptr(REF), _dptr(TRN),
                                              st.ctypes.data_as(C.POINTER(C.c_int))))
         self._stack_shape = (len(stacks), len(stacks[0]["layers"]), *np.asarray(stacks[0]["layers"][0]).shape)
+        self._stack_m = m
         return REF, TRN, st
 
     def stack_backward(self, wR: np.ndarray, wT: np.ndarray, want_thick: bool = False):
@@ -494,3 +496,15 @@ class Context:
         gt = np.zeros(shape[:2])
         self._check(self.L.vrc_stack_backward(self.h, _dptr(wR), _dptr(wT), _dptr(g), _dptr(gt)))
         return (g, gt) if want_thick else g
+
+    def stack_fields(self, ngx: int = 0, ngy: int = 0):
+        """Amplitudes (nstacks, nlayers+1, 2, n) at every interface of the last
+        stack_forward and, with ngx, ngy > 0, Ex / Ey images
+        (nstacks, nlayers+1, 2, ngy, ngx) over the period."""
+        C_, L_ = self._stack_shape[:2]
+        n = 2 * self._stack_m
+        amps = np.zeros((C_, L_ + 1, 2, n), dtype=np.complex128)
+        img = np.zeros((C_, L_ + 1, 2, ngy, ngx), dtype=np.complex128) if ngx > 0 else None
+        self._check(self.L.vrc_stack_fields(self.h, int(ngx), int(ngy), amps.ctypes.data_as(CP),
+                                            img.ctypes.data_as(CP) if img is not None else None))
+        return amps, img

@@ -126,6 +126,42 @@ __global__ void thick_adjoint_kernel(const ThickAdjDesc* __restrict__ ds, int n)
   }
 }
 
+__global__ void interface_e_kernel(const IfFieldDesc* __restrict__ ds, int n) {
+  const IfFieldDesc d = ds[blockIdx.x];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    cplx s = mk(0.0, 0.0);
+    for (int k = 0; k < n; ++k) s = cfma(d.W[(size_t)k * n + i], cadd(d.ap[k], d.am[k]), s);
+    d.e[i] = s;
+  }
+}
+
+// Ex, Ey at pixel (p, q) = sum over harmonics of e_k exp(i (alpha_k x_p + beta_k y_q))
+__global__ void field_image_kernel(const IfFieldDesc* __restrict__ ds, int m, int ngx, int ngy) {
+  const IfFieldDesc d = ds[blockIdx.y];
+  if (!d.img) return;
+  const int npix = ngx * ngy;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < npix; idx += gridDim.x * blockDim.x) {
+    const int q = idx / ngx, p = idx - q * ngx;
+    const double x = d.Lx * p / ngx, y = d.Ly * q / ngy;
+    cplx ex = mk(0.0, 0.0), ey = mk(0.0, 0.0);
+    for (int k = 0; k < m; ++k) {
+      double sn, cs;
+      sincos(d.alpha[k] * x + d.beta[k] * y, &sn, &cs);
+      const cplx ph = mk(cs, sn);
+      ex = cfma(d.e[k], ph, ex);
+      ey = cfma(d.e[m + k], ph, ey);
+    }
+    d.img[idx] = ex;
+    d.img[npix + idx] = ey;
+  }
+}
+
+__global__ void vec_axpy_kernel(const cplx* const* __restrict__ as, const cplx* const* __restrict__ bs, cplx s,
+                                cplx* const* __restrict__ ys, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) ys[blockIdx.y][i] = cfma(s, bs[blockIdx.y][i], as[blockIdx.y][i]);
+}
+
 // dL/dP, dL/dQ of Layer::waveEqnCoeff (src/rcwa/Layer.cpp:36-171, periodic)
 // -> dL/dfe11, dL/dfe22 and Z = dL/dF1 Kx + dL/dF2 Ky (F = fe33^-1 [Kx Ky]).
 __global__ void pq_adjoint_kernel(const PQAdjDesc* __restrict__ ds, int m) {
@@ -543,6 +579,24 @@ void layer_adjoint_batched(const LayerAdjDesc* d, int batch, int n, cudaStream_t
 void pq_adjoint_batched(const PQAdjDesc* d, int batch, int m, cudaStream_t st) {
   if (batch <= 0) return;
   pq_adjoint_kernel<<<grid_for((long long)m * m, batch), 256, 0, st>>>(d, m);
+  VRC_CUDA_CHECK(cudaGetLastError());
+}
+
+void interface_fields_batched(const IfFieldDesc* d, int batch, int n, int ngx, int ngy, cudaStream_t st) {
+  if (batch <= 0) return;
+  interface_e_kernel<<<batch, 256, 0, st>>>(d, n);
+  VRC_CUDA_CHECK(cudaGetLastError());
+  if (ngx > 0 && ngy > 0) {
+    field_image_kernel<<<grid_for((long long)ngx * ngy, batch), 256, 0, st>>>(d, n / 2, ngx, ngy);
+    VRC_CUDA_CHECK(cudaGetLastError());
+  }
+}
+
+void vec_axpy_batched(const cplx* const* a, const cplx* const* b, cplx s, cplx* const* y, int batch, int n,
+                      cudaStream_t st) {
+  if (batch <= 0) return;
+  dim3 grid((n + 127) / 128, batch);
+  vec_axpy_kernel<<<grid, 128, 0, st>>>(a, b, s, y, n);
   VRC_CUDA_CHECK(cudaGetLastError());
 }
 

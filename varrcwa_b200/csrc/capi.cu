@@ -671,6 +671,34 @@ int vrc_stack_backward(vrc_context* ctx, const double* wR, const double* wT, dou
   });
 }
 
+int vrc_stack_fields(vrc_context* ctx, int ngx, int ngy, vrc_complex* amps, vrc_complex* fields) {
+  return guarded(ctx, [&] {
+    if (!amps || ngx < 0 || ngy < 0 || ((ngx > 0) != (ngy > 0)) || (ngx > 0 && !fields))
+      throw vrc::StatusError(VRC_EINVAL, "invalid arguments");
+    const int G = ctx->stack_lanes;
+    const vrc::Engine::StackTape& t0 = ctx->eng->stack_tape();
+    if (t0.C == 0) throw vrc::StatusError(VRC_EINVAL, "stack fields: no forward solve");
+    const size_t pa = (size_t)(t0.L + 1) * 2 * t0.n, pi = (size_t)(t0.L + 1) * 2 * ngx * ngy;
+    int nst = 0;
+    for (int g = 0; g < G; ++g) nst += lane(ctx, g).stack_tape().C;
+    Timed tm(ctx);
+    std::vector<std::vector<cplx>> la(G), li(G);
+    for_lanes(
+        ctx, G,
+        [&](int g, vrc::Engine& E) {
+          la[g].resize((size_t)E.stack_tape().C * pa);
+          li[g].resize((size_t)E.stack_tape().C * pi);
+          E.stack_fields(ngx, ngy, la[g].data(), pi ? li[g].data() : nullptr);
+        },
+        [](int) {});
+    for (int c = 0; c < nst; ++c) {
+      std::memcpy(amps + (size_t)c * pa, la[c % G].data() + (size_t)(c / G) * pa, pa * 16);
+      if (pi) std::memcpy(fields + (size_t)c * pi, li[c % G].data() + (size_t)(c / G) * pi, pi * 16);
+    }
+    tm.done();
+  });
+}
+
 int vrc_gds_read(const char* path, double unit, int* npoly, int* npoints, int* poly_start, double* poly_xz,
                  int max_poly, int max_points) {
   if (!path || !npoly || !npoints || !(unit > 0.0)) return VRC_EINVAL;

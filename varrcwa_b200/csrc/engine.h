@@ -280,6 +280,11 @@ class Engine {
   // grad_thick (L per stack, may be null): dL/d(layer thickness).
   void stack_backward(const double* wR, const double* wT, double* grad, double* grad_thick = nullptr);
   void release_stack_tape();
+  // Up- and down-going amplitudes at every interface j = 0..L of the stacks of
+  // the last stack_forward (amps: per stack (L+1) x 2 x n, a+ then a-, in the
+  // basis of the region below the interface) and Ex, Ey on an ngx x ngy grid
+  // over the period (img: per stack (L+1) x 2 x ngy x ngx; may be null).
+  void stack_fields(int ngx, int ngy, cplx* amps, cplx* img);
 
   // counters
   long long launches = 0;

@@ -152,6 +152,19 @@ struct ThickAdjDesc {
   double k0;
 };
 void thick_adjoint_batched(const ThickAdjDesc* d, int batch, int n, cudaStream_t st);
+// Interface fields: e = W (ap + am) (one CTA per interface), then Ex, Ey on an
+// ngx x ngy grid over the period from the harmonics (index ny*i + j).
+struct IfFieldDesc {
+  const cplx *W, *ap, *am;
+  cplx* e;  // n
+  const double *alpha, *beta;
+  cplx* img;  // 2 * ngy * ngx (Ex then Ey), may be null
+  double Lx, Ly;
+};
+void interface_fields_batched(const IfFieldDesc* d, int batch, int n, int ngx, int ngy, cudaStream_t st);
+// y = a + b * s (vectors of n)
+void vec_axpy_batched(const cplx* const* a, const cplx* const* b, cplx s, cplx* const* y, int batch, int n,
+                      cudaStream_t st);
 bool pixel_adjoint_fits(int nx, int ny, int npx, int npy);
 size_t pixel_adjoint_scratch(int nx, int ny);
 void pixel_adjoint_batched(const PixAdjDesc* d, int batch, int nx, int ny, int npx, int npy, cudaStream_t st);

@@ -523,3 +523,150 @@ void Engine::stack_backward(const double* wR, const double* wT, double* grad, do
 }
 
 }  // namespace vrc
+
+namespace vrc {
+
+// Internal amplitudes (the role of RCWASolver::evaluateIntermediateField,
+// src/rcwa/RCWASolver.cpp:1373-1480) from the forward's prefix chains and
+// suffix chains formed here: at interface j (0 < j < L) between the chain S_L
+// of layers 0..j-1 and the rest S_R (layers j..L-1 and the exit, left end in
+// the basis of layer j-1),  a+ = (I - Rud_L Rdu_R)^-1 Tuu_L c,  a- = Rdu_R a+.
+void Engine::stack_fields(int ngx, int ngy, cplx* amps, cplx* img) {
+  StackTape& tp = tape_;
+  if (tp.C == 0) throw StatusError(ST_EINVAL, "stack fields: no forward solve");
+  if (ngx < 0 || ngy < 0) throw StatusError(ST_EINVAL, "stack fields: negative grid");
+  const int C = tp.C, L = tp.L, n = tp.n, m = tp.m;
+  Batch bt{*this, C};
+  auto gather = [&](auto fn) {
+    Vec v(C);
+    for (int c = 0; c < C; ++c) v[c] = fn(tp.cells[c]);
+    return v;
+  };
+  const size_t nv = (size_t)n;
+  // device vectors: per stack c, s, v, and (L+1) x (a+, a-, e)
+  const size_t per = 3 * nv + (size_t)(L + 1) * 3 * nv;
+  cplx* dv = (cplx*)bytes((size_t)C * per * 16);
+  auto cvec = [&](int c) { return dv + c * per; };
+  auto svec = [&](int c) { return dv + c * per + nv; };
+  auto tvec = [&](int c) { return dv + c * per + 2 * nv; };
+  auto ap = [&](int c, int j) { return dv + c * per + 3 * nv + (size_t)j * 3 * nv; };
+  auto am = [&](int c, int j) { return ap(c, j) + nv; };
+  auto ev = [&](int c, int j) { return ap(c, j) + 2 * nv; };
+  VRC_CUDA_CHECK(cudaMemsetAsync(dv, 0, (size_t)C * per * 16, stream_));
+  const size_t npix = (size_t)ngx * ngy;
+  cplx* dimg = npix ? (cplx*)bytes((size_t)C * (L + 1) * 2 * npix * 16) : nullptr;
+  auto matvec = [&](const std::vector<MatVecDesc>& d) {
+    Prof pr(*this, "fields", 8.0 * nv * nv * d.size(), 16.0 * nv * nv * d.size());
+    matvec_batched(upload(d), (int)d.size(), n, stream_);
+  };
+  // incidence c = W0^-1 s, s the (px, py) plane wave of the forward
+  {
+    const int ctr = (tp.ny * (tp.nx - 1)) / 2 + (tp.ny - 1) / 2;
+    std::vector<cplx> hs((size_t)C * nv, mk(0.0, 0.0));
+    for (int c = 0; c < C; ++c) {
+      hs[(size_t)c * nv + ctr] = mk(tp.px, 0.0);
+      hs[(size_t)c * nv + m + ctr] = mk(tp.py, 0.0);
+    }
+    cplx* ds = upload(hs);
+    std::vector<MatVecDesc> d(C);
+    for (int c = 0; c < C; ++c) {
+      VRC_CUDA_CHECK(cudaMemcpyAsync(svec(c), ds + (size_t)c * nv, nv * 16, cudaMemcpyDeviceToDevice, stream_));
+      d[c] = {tp.cells[c].e0.Winv, svec(c), cvec(c)};
+    }
+    matvec(d);
+  }
+  // entrance (incident, reflected) and exit (transmitted, nothing incoming)
+  {
+    std::vector<const cplx*> a, b;
+    std::vector<cplx*> y;
+    std::vector<MatVecDesc> d;
+    for (int c = 0; c < C; ++c) {
+      a.push_back(cvec(c));
+      b.push_back(cvec(c));
+      y.push_back(ap(c, 0));
+      d.push_back({tp.cells[c].S[3], cvec(c), am(c, 0)});
+      d.push_back({tp.cells[c].S[1], cvec(c), ap(c, L)});
+    }
+    vec_axpy_batched(upload(a), upload(b), mk(0.0, 0.0), upload(y), C, n, stream_);
+    matvec(d);
+  }
+  if (L > 1) {
+    // exit interface (zero thickness, left end in the last layer's basis):
+    // Tuu = Ar^-1, Rud = -Ar^-1 Br, Rdu = Br Ar^-1, Tdd = Ar - Br Ar^-1 Br
+    Vec Ar = gather([](StackCell& s) { return s.Ar; });
+    Vec Br = gather([](StackCell& s) { return s.Br; });
+    std::vector<Vec> SR(L + 1);
+    for (int j = 1; j <= L; ++j) {
+      SR[j].resize(4 * C);
+      for (auto& p : SR[j]) p = mat(n);
+    }
+    auto blk = [&](int j, int k) {
+      Vec v(C);
+      for (int c = 0; c < C; ++c) v[c] = SR[j][4 * c + k];
+      return v;
+    };
+    Vec Ai = blk(L, 1);
+    copy(Ar, Ai, n);
+    inverse(Ai, n, nullptr);
+    bt.mm(blk(L, 2), Ai, Br, MONE, 0, 0, nullptr, ZERO, n);   // Rud
+    bt.mm(blk(L, 3), Br, Ai, ONE, 0, 0, nullptr, ZERO, n);    // Rdu
+    bt.mm(blk(L, 0), Br, blk(L, 2), ONE, 0, 0, &Ar, ONE, n);  // Tdd = Ar + Br Rud
+    for (int j = L - 1; j >= 1; --j) {
+      std::vector<StarReq> sr(C);
+      for (int c = 0; c < C; ++c) {
+        const StackLayer& ly = tp.cells[c].lay[j];
+        sr[c] = {ly.seg[0], ly.seg[1], ly.seg[2], ly.seg[3], SR[j + 1][4 * c], SR[j + 1][4 * c + 1],
+                 SR[j + 1][4 * c + 2], SR[j + 1][4 * c + 3], SR[j][4 * c], SR[j][4 * c + 1], SR[j][4 * c + 2],
+                 SR[j][4 * c + 3]};
+      }
+      star(sr, n, nullptr);
+    }
+    Vec M = bt.alloc(n);
+    for (int j = 1; j < L; ++j) {
+      Vec RudL = gather([&](StackCell& s) { return s.lay[j].pre[2]; });
+      Vec RduR = blk(j, 3);
+      bt.mm(M, RudL, RduR, MONE, 0, 0, nullptr, ZERO, n, nullptr, 1.0);  // I - Rud_L Rdu_R
+      inverse(M, n, nullptr);
+      std::vector<MatVecDesc> d1(C), d2(C), d3(C);
+      for (int c = 0; c < C; ++c) d1[c] = {tp.cells[c].lay[j].pre[1], cvec(c), tvec(c)};  // Tuu_L c
+      matvec(d1);
+      for (int c = 0; c < C; ++c) d2[c] = {M[c], tvec(c), ap(c, j)};
+      matvec(d2);
+      for (int c = 0; c < C; ++c) d3[c] = {RduR[c], ap(c, j), am(c, j)};
+      matvec(d3);
+    }
+    bt.release(M, n);
+    for (int j = 1; j <= L; ++j)
+      for (auto* p : SR[j]) free_mat(p, n);
+  }
+  // transverse E harmonics and images at every interface
+  {
+    std::vector<IfFieldDesc> fd;
+    for (int c = 0; c < C; ++c)
+      for (int j = 0; j <= L; ++j) {
+        const StackCell& sc = tp.cells[c];
+        const cplx* W = j == 0 ? sc.e0.W : (j == L ? sc.e1.W : sc.lay[j - 1].W);
+        fd.push_back({W, ap(c, j), am(c, j), ev(c, j), sc.alpha, sc.beta,
+                      dimg ? dimg + ((size_t)c * (L + 1) + j) * 2 * npix : nullptr, tp.specs[c].Lx, tp.specs[c].Ly});
+      }
+    Prof pr(*this, "fields", 8.0 * nv * nv * fd.size(), 16.0 * (nv * nv + 2.0 * npix) * fd.size());
+    interface_fields_batched(upload(fd), (int)fd.size(), n, ngx, ngy, stream_);
+  }
+  // copy out: amplitudes (a+, a-) per interface, then the images
+  std::vector<cplx> ha((size_t)C * per);
+  VRC_CUDA_CHECK(cudaMemcpyAsync(ha.data(), dv, ha.size() * 16, cudaMemcpyDeviceToHost, stream_));
+  std::vector<cplx> hi(dimg ? (size_t)C * (L + 1) * 2 * npix : 0);
+  if (dimg) VRC_CUDA_CHECK(cudaMemcpyAsync(hi.data(), dimg, hi.size() * 16, cudaMemcpyDeviceToHost, stream_));
+  sync();
+  if (amps)
+    for (int c = 0; c < C; ++c)
+      for (int j = 0; j <= L; ++j) {
+        const cplx* src = ha.data() + c * per + 3 * nv + (size_t)j * 3 * nv;
+        std::memcpy(amps + ((size_t)c * (L + 1) + j) * 2 * nv, src, 2 * nv * 16);
+      }
+  if (img && dimg) std::memcpy(img, hi.data(), hi.size() * 16);
+  free_bytes(dv, (size_t)C * per * 16);
+  if (dimg) free_bytes(dimg, (size_t)C * (L + 1) * 2 * npix * 16);
+}
+
+}  // namespace vrc
