@@ -286,17 +286,26 @@ void ensure_smem(const void* kernel, size_t bytes) {
   }
 }
 
+namespace {
+// GEMM tile choices, shared by every engine of the process (the tuning of a
+// shape runs once, under the lock, even with several engines in flight)
+std::mutex g_tile_mu;
+std::map<int, int> g_tile;  // key n * 4 + opA * 2 + opB
+}  // namespace
+
 int Engine::gemm_tile_cached(int n, int opA, int opB) const {
-  auto it = gemm_tile_.find(n * 4 + opA * 2 + opB);
-  return it == gemm_tile_.end() ? 0 : it->second;
+  std::lock_guard<std::mutex> lock(g_tile_mu);
+  auto it = g_tile.find(n * 4 + opA * 2 + opB);
+  return it == g_tile.end() ? 0 : it->second;
 }
 
 int Engine::gemm_tile(int n, int opA, int opB, size_t batch) {
   if (const char* e = std::getenv("VRC_GEMM_TILE")) return std::atoi(e) == 32 ? 32 : 64;
   if (n > 192) return 64;  // the 64-wide tile pads at most 25% there
   const int key = n * 4 + opA * 2 + opB;
-  auto it = gemm_tile_.find(key);
-  if (it != gemm_tile_.end()) return it->second;
+  std::lock_guard<std::mutex> lock(g_tile_mu);
+  auto it = g_tile.find(key);
+  if (it != g_tile.end()) return it->second;
   if (batch < 64) return 64;  // tune on a batch that fills the GPU
   // time both tiles on zeroed scratch operands (a real call may update its
   // output in place, so it cannot be run twice)
@@ -325,7 +334,7 @@ int Engine::gemm_tile(int n, int opA, int opB, size_t batch) {
   for (auto* p : m3) free_mat(p, n);
   launches += 8;
   const int best = ms[1] < ms[0] ? 32 : 64;
-  gemm_tile_[key] = best;
+  g_tile[key] = best;
   return best;
 }
 

@@ -135,8 +135,9 @@ class Engine {
   // opA / opB = 1: that operand enters as its conjugate transpose.
   void gemm(std::vector<GemmDesc>& d, int n, cplx alpha, cplx beta, double delta, int opA = 0, int opB = 0);
   // GEMM tile for order n and operand modes: timed once per shape on scratch
-  // operands (both tiles give identical results) and cached; VRC_GEMM_TILE
-  // forces one.  0 from gemm_tile_cached when the shape was not tuned yet.
+  // operands (both tiles give identical results) and cached for the whole
+  // process; VRC_GEMM_TILE forces one.  0 from gemm_tile_cached when the
+  // shape was not tuned yet.
   int gemm_tile(int n, int opA, int opB, size_t batch);
   int gemm_tile_cached(int n, int opA, int opB) const;
   void inverse(const std::vector<cplx*>& mats, int n, std::vector<int>* status);
@@ -380,7 +381,6 @@ class Engine {
 
  private:
   StackTape tape_;
-  std::map<int, int> gemm_tile_;  // key n * 4 + opA * 2 + opB
 };
 
 template <class T>
