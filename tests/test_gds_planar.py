@@ -117,3 +117,21 @@ def test_planar_section_two_polygons_and_shift():
     ox, oeps = o.section(1.0)
     np.testing.assert_array_equal(x, ox)
     np.testing.assert_array_equal(eps, oeps)
+
+
+def test_planar_straight_waveguide_known_answer():
+    """A z-invariant planar device (one straight strip): the oracle's varRCWA
+    accepts the whole range as one segment, and its S-matrix equals a single
+    RCWA slab of the same cross-section (the z-invariance known answer on the
+    GDSIISampler path)."""
+    from oracle import varrcwa_oracle as O
+    from oracle.structures_adapter import make_sampler
+    d = st.planar_taper(w0=0.5, w1=0.5, length=1.0, norders=(5, 3))
+    s = make_sampler(d)
+    S = O.redheffer_compute(s, d["z0"], d["z1"], pe=1e-8)
+    assert S.N == 1
+    R = O.rcwa_compute(s, d["z0"], d["z1"], 1)
+    F, G = S.fourier_blocks(), R.fourier_blocks()
+    scale = np.linalg.norm(G["Tuu"])  # the reflections vanish (own end bases)
+    for k in F:
+        assert np.linalg.norm(F[k] - G[k]) <= 1e-9 * scale, k
