@@ -1,0 +1,126 @@
+"""CPU restatement of a geometric-parameter gradient for adaptive varRCWA
+cells on a fixed segmentation (the accepted leaves of the adaptive tree).
+
+TEST INFRASTRUCTURE ONLY: the GPU path never imports this module.  It states
+the algorithm the device adjoint of adaptive cells is to follow and pins it
+against central differences of the oracle's own forward on the same cuts.
+
+Forward: redheffer_segments (the trisecting integrator's accepted segments,
+src/core/RedhefferIntegrator.cpp:174-399), each segment the first-order
+perturbative S-matrix in the eigenbasis of its midpoint sample, its left end
+re-expressed in the previous segment's basis, star-multiplied, the right end
+moved to the end basis.
+
+Gradient: every basis is held fixed (a fixed basis re-expresses the same
+operator exactly), so a parameter reaches the S-matrix through the samples
+P(z), Q(z) inside each segment only, and to first order by the segment
+formula itself applied to dP/dtheta, dQ/dtheta at its three Simpson nodes
+(the reference sample included: the basis is frozen, the sample moves).
+The chain is reversed with respect to the segment blocks (star products and
+projections, as for layer stacks).  dP/dtheta of a sample is taken here by
+central differences of the sampler (assembly only, no eigen-solve).
+
+Scope: parameters that leave the two end cross-sections unchanged (the end
+bases are then fixed too).  A parameter that moves an end also moves the end
+basis the result is expressed in; that term is not included.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import varrcwa_oracle as O
+from .stack_adjoint import H, project_left_adjoint, project_right_adjoint, star_adjoint
+
+
+def segments_forward(sampler, cuts):
+    """redheffer_segments with the quantities the reverse pass needs."""
+    k0 = sampler.k0
+    cuts = list(cuts)
+    P0, Q0 = sampler.sample(cuts[0])
+    b0 = O.Basis(*O.wave_equation_solve(P0, Q0))
+    P1, Q1 = sampler.sample(cuts[-1])
+    b1 = O.Basis(*O.wave_equation_solve(P1, Q1))
+    n = P0.shape[0]
+    I = np.eye(n, dtype=np.complex128)
+    Z = np.zeros((n, n), np.complex128)
+    S = [I.copy(), I.copy(), Z.copy(), Z.copy()]
+    leftW, leftV = b0.W, b0.V
+    tape = []
+    Pa, Qa = P0, Q0
+    for a, b in zip(cuts[:-1], cuts[1:]):
+        Pm, Qm = sampler.sample(0.5 * (a + b))
+        Pb, Qb = (P1, Q1) if b == cuts[-1] else sampler.sample(b)
+        bm = O.Basis(*O.wave_equation_solve(Pm, Qm))
+        seg, _ = O.perturbation_segment(Pm, Qm, bm, k0, a, b, (Pa, Pm, Pb), (Qa, Qm, Qb))
+        invW, invV = bm.solveW(leftW), bm.solveV(leftV)
+        A, B = 0.5 * (invW + invV), 0.5 * (invW - invV)
+        segp = O.project_left(seg, bm, leftW, leftV)
+        tape.append(dict(a=a, b=b, basis=bm, seg=seg, segp=segp,
+                         ABM=(A, B, np.linalg.inv(A - seg[3] @ B)), prefix=S))
+        S = O.star_right(S, segp)
+        leftW, leftV = bm.W, bm.V
+        Pa, Qa = Pb, Qb
+    Sc = S
+    Ar = 0.5 * (np.linalg.solve(leftW, b1.W) + np.linalg.solve(leftV, b1.V))
+    Br = 0.5 * (np.linalg.solve(leftW, b1.W) - np.linalg.solve(leftV, b1.V))
+    S = O.project_right(Sc, leftW, leftV, b1.W, b1.V)
+    return dict(tape=tape, Sc=Sc, S=S, ABr=(Ar, Br, np.linalg.inv(Ar - Sc[2] @ Br)), b0=b0, b1=b1, k0=k0)
+
+
+def first_order_blocks(basis, k0, a, b, dP3, dQ3):
+    """The segment formula (RedhefferIntegrator.cpp:343-396) applied to
+    perturbations dP3, dQ3 at (a, midpoint, b) in a fixed basis: the
+    segment's own-basis blocks' first-order change."""
+    W, V, gam = basis.W, basis.V, basis.gam
+    dA, dB = [], []
+    for dP, dQ in zip(dP3, dQ3):
+        x = basis.solveW(dP @ V)
+        y = basis.solveV(dQ @ W)
+        dA.append(x + y)
+        dB.append(x - y)
+    dz = b - a
+    ph = np.exp(1j * 0.5 * dz / k0 * gam)
+    pf = np.exp(1j * dz / k0 * gam)
+    c = 1j * dz / (12 * k0)
+    tuu = c * (pf[:, None] * dA[0] + 4.0 * ph[:, None] * dA[1] * ph[None, :] + dA[2] * pf[None, :])
+    rud = -c * (pf[:, None] * dB[0] * pf[None, :] + 4.0 * ph[:, None] * dB[1] * ph[None, :] + dB[2])
+    rdu = -c * (dB[0] + 4.0 * ph[:, None] * dB[1] * ph[None, :] + pf[:, None] * dB[2] * pf[None, :])
+    tdd = c * (dA[0] * pf[None, :] + 4.0 * ph[:, None] * dA[1] * ph[None, :] + pf[:, None] * dA[2])
+    return [tdd, tuu, rud, rdu]
+
+
+def segments_block_adjoints(fw, gS):
+    """Own-basis block adjoints of every segment from the adjoints gS of the
+    final blocks (Tdd, Tuu, Rud, Rdu)."""
+    G = project_right_adjoint(fw["Sc"], fw["ABr"], fw["S"], gS)
+    out = [None] * len(fw["tape"])
+    for j in range(len(fw["tape"]) - 1, -1, -1):
+        t = fw["tape"][j]
+        G, gsegp = star_adjoint(t["prefix"], t["segp"], G)
+        out[j] = project_left_adjoint(t["seg"], t["ABM"], t["segp"], gsegp)
+    return out
+
+
+def segments_gradient(fw, gS, dsample):
+    """dL/dtheta for one parameter: gS are the adjoints of the final blocks,
+    dsample(z) -> (dP/dtheta, dQ/dtheta) at a sample position."""
+    gsegs = segments_block_adjoints(fw, gS)
+    grad = 0.0
+    for t, g in zip(fw["tape"], gsegs):
+        a, b = t["a"], t["b"]
+        dd = [dsample(a), dsample(0.5 * (a + b)), dsample(b)]
+        ds = first_order_blocks(t["basis"], fw["k0"], a, b, [x[0] for x in dd], [x[1] for x in dd])
+        grad += sum(float(np.real(np.vdot(gi, di))) for gi, di in zip(g, ds))
+    return grad
+
+
+def fourier_transmission_adjoint(fw, k):
+    """Adjoint of L = |(W1 Tuu W0^-1)[k, k]|^2 (power of Fourier harmonic k
+    carried through) with respect to the final Tuu; other blocks zero."""
+    n = fw["S"][0].shape[0]
+    W0i = np.linalg.inv(fw["b0"].W)
+    Tf = fw["b1"].W @ fw["S"][1] @ W0i
+    gTf = np.zeros((n, n), np.complex128)
+    gTf[k, k] = 2.0 * Tf[k, k]
+    Z = np.zeros((n, n), np.complex128)
+    return float(abs(Tf[k, k]) ** 2), [Z, H(fw["b1"].W) @ gTf @ H(W0i), Z, Z.copy()]
