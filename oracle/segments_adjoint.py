@@ -20,9 +20,12 @@ The chain is reversed with respect to the segment blocks (star products and
 projections, as for layer stacks).  dP/dtheta of a sample is taken here by
 central differences of the sampler (assembly only, no eigen-solve).
 
-Scope: parameters that leave the two end cross-sections unchanged (the end
-bases are then fixed too).  A parameter that moves an end also moves the end
-basis the result is expressed in; that term is not included.
+A parameter that moves an end cross-section also moves the end basis the
+result is expressed in (the semi-infinite continuation of that section):
+end_bases_adjoint reverses the two end projections and the objective with
+respect to the end bases (W, V), to be contracted with dW/dtheta, dV/dtheta of
+the end eigen-decompositions (end_basis_derivative: central differences
+with the eigenvectors' order and phase aligned to the unperturbed basis).
 """
 from __future__ import annotations
 
@@ -89,23 +92,108 @@ def first_order_blocks(basis, k0, a, b, dP3, dQ3):
     return [tdd, tuu, rud, rdu]
 
 
-def segments_block_adjoints(fw, gS):
+def segments_block_adjoints(fw, gS, want_first=False):
     """Own-basis block adjoints of every segment from the adjoints gS of the
-    final blocks (Tdd, Tuu, Rud, Rdu)."""
+    final blocks (Tdd, Tuu, Rud, Rdu); with want_first also the adjoints of
+    the first segment's projected blocks (for the entrance-basis term)."""
     G = project_right_adjoint(fw["Sc"], fw["ABr"], fw["S"], gS)
     out = [None] * len(fw["tape"])
+    first = None
     for j in range(len(fw["tape"]) - 1, -1, -1):
         t = fw["tape"][j]
         G, gsegp = star_adjoint(t["prefix"], t["segp"], G)
         out[j] = project_left_adjoint(t["seg"], t["ABM"], t["segp"], gsegp)
-    return out
+        if j == 0:
+            first = gsegp
+    return (out, first) if want_first else out
 
 
-def segments_gradient(fw, gS, dsample):
+def _proj_left_ab_adjoint(s, ABM, sn, G):
+    """Reverse of project_left with respect to its projection matrices A, B
+    (segment blocks s fixed)."""
+    tdd, tuu, rud, rdu = s
+    tdd_n, tuu_n, rud_n, rdu_n = sn
+    gtdd_n, gtuu_n, grud_n, grdu_n = G
+    A, B, Minv = ABM
+    tB = tuu @ B
+    gA = H(tuu) @ gtuu_n
+    gB = H(tuu) @ gtuu_n @ H(rdu_n) + H(tuu) @ grud_n @ H(tdd_n)
+    grdu_n2 = grdu_n + H(tB) @ gtuu_n
+    gtdd_n2 = gtdd_n + H(tB) @ grud_n
+    gY = H(Minv) @ grdu_n2
+    gM = -H(Minv) @ gtdd_n2 @ H(tdd_n) - gY @ H(rdu_n)
+    gA = gA + H(rdu) @ gY + gM
+    gB = gB - gY - H(rdu) @ gM
+    return gA, gB
+
+
+def _proj_right_ab_adjoint(S, ABr, Sn, G):
+    """Reverse of project_right with respect to its projection matrices."""
+    Tdd, Tuu, Rud, Rdu = S
+    Tdd_n, Tuu_n, Rud_n, Rdu_n = Sn
+    gTdd_n, gTuu_n, gRud_n, gRdu_n = G
+    A, B, Minv = ABr
+    TB = Tdd @ B
+    gTuu_n2 = gTuu_n + H(TB) @ gRdu_n
+    gRud_n2 = gRud_n + H(TB) @ gTdd_n
+    gB = H(Tdd) @ gRdu_n @ H(Tuu_n) + H(Tdd) @ gTdd_n @ H(Rud_n)
+    gA = H(Tdd) @ gTdd_n
+    gY = H(Minv) @ gRud_n2
+    gM = -H(Minv) @ gTuu_n2 @ H(Tuu_n) - gY @ H(Rud_n)
+    gA = gA + H(Rud) @ gY + gM
+    gB = gB - gY - H(Rud) @ gM
+    return gA, gB
+
+
+def end_bases_adjoint(fw, gS, gsegp_first, gW0_obj=None, gW1_obj=None):
+    """dL/d(W0, V0, W1, V1) of the end bases through the entrance projection
+    of the first segment and the exit projection (plus explicit objective
+    terms).  A = (L_W^-1 W + L_V^-1 V) / 2, B = (L_W^-1 W - L_V^-1 V) / 2."""
+    t0 = fw["tape"][0]
+    gA, gB = _proj_left_ab_adjoint(t0["seg"], t0["ABM"], t0["segp"], gsegp_first)
+    bm = t0["basis"]
+    Wi, Vi = np.linalg.inv(bm.W), np.linalg.inv(bm.V)
+    gW0 = 0.5 * H(Wi) @ (gA + gB)
+    gV0 = 0.5 * H(Vi) @ (gA - gB)
+    gA, gB = _proj_right_ab_adjoint(fw["Sc"], fw["ABr"], fw["S"], gS)
+    last = fw["tape"][-1]["basis"]
+    Wi, Vi = np.linalg.inv(last.W), np.linalg.inv(last.V)
+    gW1 = 0.5 * H(Wi) @ (gA + gB)
+    gV1 = 0.5 * H(Vi) @ (gA - gB)
+    if gW0_obj is not None:
+        gW0 = gW0 + gW0_obj
+    if gW1_obj is not None:
+        gW1 = gW1 + gW1_obj
+    return gW0, gV0, gW1, gV1
+
+
+def end_basis_derivative(sampler_p, sampler_m, z, ref, h):
+    """dW/dtheta, dV/dtheta of the eigenbasis at z by central differences of
+    the sampler, each perturbed basis's columns matched to `ref` by overlap
+    and their phases aligned (the zgeev normalisation fixes each column only
+    up to a phase, which the S-matrix's end projections absorb)."""
+    out = []
+    for smp in (sampler_p, sampler_m):
+        P, Q = smp.sample(z)
+        W, V, _ = O.wave_equation_solve(P, Q)
+        idx = np.argmax(np.abs(H(ref.W) @ W), axis=1)
+        W, V = W[:, idx], V[:, idx]
+        ph = np.array([np.vdot(W[:, i], ref.W[:, i]) for i in range(W.shape[1])])
+        ph = ph / np.abs(ph)
+        out.append((W * ph[None, :], V * ph[None, :]))
+    return (out[0][0] - out[1][0]) / (2 * h), (out[0][1] - out[1][1]) / (2 * h)
+
+
+def segments_gradient(fw, gS, dsample, end_terms=None):
     """dL/dtheta for one parameter: gS are the adjoints of the final blocks,
-    dsample(z) -> (dP/dtheta, dQ/dtheta) at a sample position."""
+    dsample(z) -> (dP/dtheta, dQ/dtheta) at a sample position.  end_terms:
+    optional ((gW0, gV0, gW1, gV1), (dW0, dV0, dW1, dV1)) for a parameter that
+    moves an end cross-section."""
     gsegs = segments_block_adjoints(fw, gS)
     grad = 0.0
+    if end_terms is not None:
+        for g, dv in zip(*end_terms):
+            grad += float(np.real(np.vdot(g, dv)))
     for t, g in zip(fw["tape"], gsegs):
         a, b = t["a"], t["b"]
         dd = [dsample(a), dsample(0.5 * (a + b)), dsample(b)]
@@ -114,13 +202,20 @@ def segments_gradient(fw, gS, dsample):
     return grad
 
 
-def fourier_transmission_adjoint(fw, k):
+def fourier_transmission_adjoint(fw, k, want_bases=False):
     """Adjoint of L = |(W1 Tuu W0^-1)[k, k]|^2 (power of Fourier harmonic k
-    carried through) with respect to the final Tuu; other blocks zero."""
+    carried through) with respect to the final Tuu; other blocks zero.  With
+    want_bases also the explicit dL/dW0 and dL/dW1 of the Fourier mapping."""
     n = fw["S"][0].shape[0]
     W0i = np.linalg.inv(fw["b0"].W)
-    Tf = fw["b1"].W @ fw["S"][1] @ W0i
+    Tuu = fw["S"][1]
+    Tf = fw["b1"].W @ Tuu @ W0i
     gTf = np.zeros((n, n), np.complex128)
     gTf[k, k] = 2.0 * Tf[k, k]
     Z = np.zeros((n, n), np.complex128)
-    return float(abs(Tf[k, k]) ** 2), [Z, H(fw["b1"].W) @ gTf @ H(W0i), Z, Z.copy()]
+    out = (float(abs(Tf[k, k]) ** 2), [Z, H(fw["b1"].W) @ gTf @ H(W0i), Z, Z.copy()])
+    if not want_bases:
+        return out
+    gW1 = gTf @ H(Tuu @ W0i)
+    gW0 = -H(W0i) @ H(fw["b1"].W @ Tuu) @ gTf @ H(W0i)
+    return out + (gW0, gW1)

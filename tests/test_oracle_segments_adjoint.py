@@ -3,9 +3,11 @@ segmentation (oracle/segments_adjoint.py): the frozen-basis first-order
 adjoint against central differences of the oracle's forward on the same cuts,
 for a control knot inside the cell (the end cross-sections unchanged)."""
 import numpy as np
+import pytest
 
 from oracle import varrcwa_oracle as O
-from oracle.segments_adjoint import fourier_transmission_adjoint, segments_forward, segments_gradient
+from oracle.segments_adjoint import (end_bases_adjoint, end_basis_derivative, fourier_transmission_adjoint,
+                                     segments_block_adjoints, segments_forward, segments_gradient)
 from oracle.structures_adapter import make_sampler
 from varrcwa_b200 import structures as st
 
@@ -50,3 +52,50 @@ def test_interior_knot_gradient_matches_central_differences():
     # truncation (1.8e-6 at pe = 1e-6, 5.7e-6 here)
     assert abs(g - fd) <= 2e-5 * abs(fd), (g, fd)
     assert abs(J - objective(knot)) < 1e-14
+
+
+def _cell_end(kv, which):
+    """The taper with an off-centre middle knot; knot `which` (0: z0, 2: z1)
+    of the right core edge takes the value kv."""
+    d = dict(st.taper_2d(norders=11))
+    (i1, zs1, v1), (i2, zs2, v2) = d["xrules"]
+    L = zs2[-1]
+    v = [v2[0], 0.5 * (v2[0] + v2[1]) + 0.05, v2[1]]
+    v[which] = kv
+    d["xrules"] = [(i1, [0.0, 0.5 * L, L], [v1[0], 0.5 * (v1[0] + v1[1]), v1[1]]), (i2, [0.0, 0.5 * L, L], v)]
+    return d
+
+
+@pytest.mark.parametrize("which", [0, 2])
+def test_end_knot_gradient_with_end_basis_terms(which):
+    """A knot that moves an end cross-section: the segment terms plus the
+    derivative through that end's eigenbasis meet central differences."""
+    base = st.taper_2d(norders=11)["xrules"][1][2]
+    kv = (base[1] if which == 2 else base[0]) + 0.02
+    d = _cell_end(kv, which)
+    s = make_sampler(d)
+    cuts = O.tree_cuts(O.redheffer_compute(s, d["z0"], d["z1"], pe=1e-5).nodes)
+    fw = segments_forward(s, cuts)
+    k = 5
+    J, gS, gW0o, gW1o = fourier_transmission_adjoint(fw, k, want_bases=True)
+    _, gfirst = segments_block_adjoints(fw, gS, want_first=True)
+    gends = end_bases_adjoint(fw, gS, gfirst, gW0o, gW1o)
+    h = 1e-6
+    sp, sm = make_sampler(_cell_end(kv + h, which)), make_sampler(_cell_end(kv - h, which))
+
+    def dsample(z):
+        Pp, Qp = sp.sample(z)
+        Pm, Qm = sm.sample(z)
+        return (Pp - Pm) / (2 * h), (Qp - Qm) / (2 * h)
+
+    dW0, dV0 = end_basis_derivative(sp, sm, d["z0"], fw["b0"], h)
+    dW1, dV1 = end_basis_derivative(sp, sm, d["z1"], fw["b1"], h)
+    g = segments_gradient(fw, gS, dsample, end_terms=(gends, (dW0, dV0, dW1, dV1)))
+
+    def objective(v):
+        f = segments_forward(make_sampler(_cell_end(v, which)), cuts)
+        return fourier_transmission_adjoint(f, k)[0]
+
+    hf = 1e-5
+    fd = (objective(kv + hf) - objective(kv - hf)) / (2 * hf)
+    assert abs(g - fd) <= 2e-5 * abs(fd), (g, fd)
