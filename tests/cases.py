@@ -51,6 +51,7 @@ CASES = {
     "pillar_pq": dict(desc=_pillar(npix=32, nord=5), pq_z=[0.1, 0.45]),
     "pml_pq": dict(desc=_pml_short(), pq_z=[0.0, 1.3]),
     "cross_pq": dict(desc=_cross_grid(), pq_z=[0.0]),
+    "planar_pq": dict(desc=st.planar_taper(norders=(5, 3)), pq_z=[0.3, 2.9]),
     "taper_redheffer": dict(desc=_taper_short(), method="redheffer", pe=1e-4),
     "pillar_rcwa": dict(desc=_pillar(), method="rcwa", N=4),
     "pillar_redheffer": dict(desc=_pillar(), method="redheffer", pe=1e-2),

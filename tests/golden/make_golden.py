@@ -6,7 +6,7 @@ oracle's outputs on small seeded structures of each benchmark family.  They
 pin the oracle against drift (tests/test_golden_oracle.py) and give the GPU
 parity tests fixed targets.
 
-Run from the repository root:  python tests/golden/make_golden.py
+Run from the repository root:  python tests/golden/make_golden.py [names...]
 """
 from __future__ import annotations
 
@@ -30,8 +30,28 @@ def fourier(S):
     return {f"F_{k}": v for k, v in F.items()}
 
 
-def main():
+def stack_small():
+    """A two-layer pixel stack: per-order powers and the pixel and thickness
+    gradients of T(+1, 0) (oracle/stack_adjoint.py)."""
+    from oracle.stack_adjoint import Stack, order_index, stack_backward, stack_forward
+    from varrcwa_b200.structures import smooth_pixels
+    layers = [smooth_pixels([4900, l], 8, 8, sigma=1.0) for l in range(2)]
+    st = Stack(0.633, 3, 3, 0.6, 0.6, layers, [0.15, 0.2], eps_in=1.0, eps_out=2.085)
+    R, T, tp = stack_forward(st)
+    wT = np.zeros(9)
+    wT[order_index(3, 3, 1, 0)] = 1.0
+    g, gt = stack_backward(st, tp, np.zeros(9), wT, want_thick=True)
+    return dict(layers=np.array(layers), R=R, T=T, grad=np.array(g), grad_thick=gt)
+
+
+def main(names=None):
+    if names is None or "stack_small" in names:
+        data = stack_small()
+        np.savez_compressed(OUT / "stack_small.npz", **data)
+        print("stack_small", {k: v.shape for k, v in data.items()})
     for name, case in CASES.items():
+        if names is not None and name not in names:
+            continue
         d = case["desc"]
         s = make_sampler(d)
         e0, e1 = end_bases(d, s)
@@ -73,4 +93,5 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    # optional fixture names: regenerate only those
+    main(sys.argv[1:] or None)

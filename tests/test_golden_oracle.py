@@ -36,3 +36,18 @@ def test_oracle_smatrix_matches_golden(name):
     F = S.fourier_blocks()
     for k in F:
         assert relerr(F[k], g["F_" + k]) < 1e-11
+
+
+def test_oracle_stack_adjoint_matches_golden():
+    """The layer-stack forward and its pixel / thickness gradients reproduce
+    the committed fixture (guards the adjoint oracle against drift)."""
+    from oracle.stack_adjoint import Stack, order_index, stack_backward, stack_forward
+    g = golden("stack_small")
+    st = Stack(0.633, 3, 3, 0.6, 0.6, list(g["layers"]), [0.15, 0.2], eps_in=1.0, eps_out=2.085)
+    R, T, tp = stack_forward(st)
+    assert np.abs(R - g["R"]).max() < 1e-13 and np.abs(T - g["T"]).max() < 1e-13
+    wT = np.zeros(9)
+    wT[order_index(3, 3, 1, 0)] = 1.0
+    gr, gt = stack_backward(st, tp, np.zeros(9), wT, want_thick=True)
+    assert relerr(np.array(gr), g["grad"]) < 1e-11
+    assert relerr(gt, g["grad_thick"]) < 1e-11
