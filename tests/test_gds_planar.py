@@ -135,3 +135,22 @@ def test_planar_straight_waveguide_known_answer():
     scale = np.linalg.norm(G["Tuu"])  # the reflections vanish (own end bases)
     for k in F:
         assert np.linalg.norm(F[k] - G[k]) <= 1e-9 * scale, k
+
+
+def test_gds_reader_units_negative_coordinates_and_skipped_elements(tmp_path):
+    """Database unit 0.1 nm, negative coordinates, TEXT and SREF elements
+    (skipped) between polygons."""
+    tri = [(-12345, -6789), (40000, -6789), (0, 55555)]
+    lib = _rec(0x00, 0x02, struct.pack(">h", 600)) + _rec(0x01, 0x02, bytes(24)) + _rec(0x02, 0x06, b"L\0")
+    lib += _rec(0x03, 0x05, _real8(1e-10 / 1e-6) + _real8(1e-10))
+    lib += _rec(0x05, 0x02, bytes(24)) + _rec(0x06, 0x06, b"T\0")
+    lib += _rec(0x0C, 0x00) + _rec(0x0D, 0x02, struct.pack(">h", 5)) + _rec(0x16, 0x02, struct.pack(">h", 0))
+    lib += _xy([(1, 2)]) + _rec(0x19, 0x06, b"hi") + _rec(0x11, 0x00)            # TEXT
+    lib += _rec(0x0A, 0x00) + _rec(0x12, 0x06, b"X\0") + _xy([(0, 0)]) + _rec(0x11, 0x00)  # SREF
+    lib += _rec(0x08, 0x00) + _rec(0x0D, 0x02, struct.pack(">h", 1)) + _rec(0x0E, 0x02, struct.pack(">h", 0))
+    lib += _xy(tri + [tri[0]]) + _rec(0x11, 0x00)
+    lib += _rec(0x07, 0x00) + _rec(0x04, 0x00)
+    (tmp_path / "u.gds").write_bytes(lib)
+    polys = capi.gds_read(tmp_path / "u.gds")
+    assert len(polys) == 1
+    np.testing.assert_allclose(polys[0], np.array(tri) * 1e-4, rtol=1e-15, atol=1e-18)
