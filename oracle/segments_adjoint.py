@@ -145,7 +145,7 @@ def _proj_right_ab_adjoint(S, ABr, Sn, G):
     return gA, gB
 
 
-def end_bases_adjoint(fw, gS, gsegp_first, gW0_obj=None, gW1_obj=None):
+def end_bases_adjoint(fw, gS, gsegp_first, gW0_obj=None, gW1_obj=None, gV0_obj=None, gV1_obj=None):
     """dL/d(W0, V0, W1, V1) of the end bases through the entrance projection
     of the first segment and the exit projection (plus explicit objective
     terms).  A = (L_W^-1 W + L_V^-1 V) / 2, B = (L_W^-1 W - L_V^-1 V) / 2."""
@@ -164,6 +164,10 @@ def end_bases_adjoint(fw, gS, gsegp_first, gW0_obj=None, gW1_obj=None):
         gW0 = gW0 + gW0_obj
     if gW1_obj is not None:
         gW1 = gW1 + gW1_obj
+    if gV0_obj is not None:
+        gV0 = gV0 + gV0_obj
+    if gV1_obj is not None:
+        gV1 = gV1 + gV1_obj
     return gW0, gV0, gW1, gV1
 
 
@@ -219,3 +223,41 @@ def fourier_transmission_adjoint(fw, k, want_bases=False):
     gW1 = gTf @ H(Tuu @ W0i)
     gW0 = -H(W0i) @ H(fw["b1"].W @ Tuu) @ gTf @ H(W0i)
     return out + (gW0, gW1)
+
+
+def mode_flux(W, V, j):
+    """z-power flux of mode j of a basis: Re sum(e_x conj(h_y) - e_y conj(h_x))
+    over the harmonics, e = W[:, j], h = V[:, j] (the interface fields'
+    flux, conserved across interfaces of lossless stacks)."""
+    m = W.shape[0] // 2
+    e, h = W[:, j], V[:, j]
+    return float(np.real(np.vdot(h[m:], e[:m]) - np.vdot(h[:m], e[m:])))
+
+
+def mode_conversion_adjoint(fw, i0, i1):
+    """L = |Tuu[i1, i0]|^2 f1 / f0: power carried from mode i0 of the entrance
+    basis into mode i1 of the exit basis, f the modes' fluxes.  Returns
+    (L, adjoints of the final blocks, dL/dW0, dL/dV0, dL/dW1, dL/dV1 of the
+    explicit flux terms)."""
+    b0, b1 = fw["b0"], fw["b1"]
+    n = b0.W.shape[0]
+    m = n // 2
+    T = fw["S"][1][i1, i0]
+    f0, f1 = mode_flux(b0.W, b0.V, i0), mode_flux(b1.W, b1.V, i1)
+    L = float(abs(T) ** 2 * f1 / f0)
+    Z = np.zeros((n, n), np.complex128)
+    gTuu = Z.copy()
+    gTuu[i1, i0] = 2.0 * T * f1 / f0
+    gS = [Z, gTuu, Z.copy(), Z.copy()]
+
+    def flux_grads(W, V, j, c):
+        gW, gV = Z.copy(), Z.copy()
+        gW[:m, j] = c * V[m:, j]
+        gW[m:, j] = -c * V[:m, j]
+        gV[:m, j] = -c * W[m:, j]
+        gV[m:, j] = c * W[:m, j]
+        return gW, gV
+
+    gW1, gV1 = flux_grads(b1.W, b1.V, i1, abs(T) ** 2 / f0)
+    gW0, gV0 = flux_grads(b0.W, b0.V, i0, -abs(T) ** 2 * f1 / f0 ** 2)
+    return L, gS, gW0, gV0, gW1, gV1

@@ -12,6 +12,14 @@ from oracle.structures_adapter import make_sampler
 from varrcwa_b200 import structures as st
 
 
+@pytest.fixture(autouse=True, scope="module")
+def _one_blas_thread():
+    # the matrices here are small (n <= 50): threaded BLAS only adds overhead
+    from threadpoolctl import threadpool_limits
+    with threadpool_limits(1):
+        yield
+
+
 def _cell(knot):
     """Config-1 style taper (11 orders) whose right core edge has a middle
     control knot at z = L/2 of value `knot` (the ends stay at w0, w1)."""
@@ -99,3 +107,61 @@ def test_end_knot_gradient_with_end_basis_terms(which):
     hf = 1e-5
     fd = (objective(kv + hf) - objective(kv - hf)) / (2 * hf)
     assert abs(g - fd) <= 2e-5 * abs(fd), (g, fd)
+
+
+def _waveguide(widths):
+    """PML waveguide mode converter (5 x 5 orders, six width control points
+    over 3 um): the widths move both core edges."""
+    d = dict(st.waveguide_pml(5000, norders=5, ncontrol=6, length=3.0))
+    zs = d["xrules"][0][1]
+    cx = 2.0
+    w = np.asarray(widths, dtype=float)
+    d["xrules"] = [(2, zs, cx - 0.5 * w), (3, zs, cx + 0.5 * w)]
+    d["x"] = np.array(d["x"])
+    d["x"][2], d["x"][3] = cx - 0.5 * w[0], cx + 0.5 * w[0]
+    return d
+
+
+@pytest.mark.parametrize("k", [2, 5])
+def test_mode_conversion_gradient_pml_waveguide(k):
+    """Config-5 style objective: power from the entrance's leading mode into
+    another mode of the exit basis, flux normalised, with respect to a width
+    control point (interior, and the exit one that moves the end basis)."""
+    from oracle.segments_adjoint import H, mode_conversion_adjoint
+    w = np.array(st.waveguide_pml(5000, norders=5, ncontrol=6, length=3.0)["widths"])
+    d = _waveguide(w)
+    s = make_sampler(d)
+    cuts = O.tree_cuts(O.redheffer_compute(s, d["z0"], d["z1"], pe=1e-4).nodes)
+    fw = segments_forward(s, cuts)
+    i0 = int(np.argmax(fw["b0"].gam.real))
+    i1 = int(np.argsort(-fw["b1"].gam.real)[1])
+    L, gS, gW0o, gV0o, gW1o, gV1o = mode_conversion_adjoint(fw, i0, i1)
+    _, gfirst = segments_block_adjoints(fw, gS, want_first=True)
+    gends = end_bases_adjoint(fw, gS, gfirst, gW0o, gW1o, gV0o, gV1o)
+    h = 1e-6
+    wp, wm = w.copy(), w.copy()
+    wp[k] += h
+    wm[k] -= h
+    sp, sm = make_sampler(_waveguide(wp)), make_sampler(_waveguide(wm))
+
+    def dsample(z):
+        Pp, Qp = sp.sample(z)
+        Pm, Qm = sm.sample(z)
+        return (Pp - Pm) / (2 * h), (Qp - Qm) / (2 * h)
+
+    dW0, dV0 = end_basis_derivative(sp, sm, d["z0"], fw["b0"], h)
+    dW1, dV1 = end_basis_derivative(sp, sm, d["z1"], fw["b1"], h)
+    g = segments_gradient(fw, gS, dsample, end_terms=(gends, (dW0, dV0, dW1, dV1)))
+
+    def objective(widths):
+        f = segments_forward(make_sampler(_waveguide(widths)), cuts)
+        j0 = int(np.argmax(np.abs(H(f["b0"].W) @ fw["b0"].W[:, i0])))
+        j1 = int(np.argmax(np.abs(H(f["b1"].W) @ fw["b1"].W[:, i1])))
+        return mode_conversion_adjoint(f, j0, j1)[0]
+
+    hf = 1e-5
+    wp, wm = w.copy(), w.copy()
+    wp[k] += hf
+    wm[k] -= hf
+    fd = (objective(wp) - objective(wm)) / (2 * hf)
+    assert abs(g - fd) <= 1e-5 * abs(fd), (g, fd)
