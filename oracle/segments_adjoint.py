@@ -261,3 +261,63 @@ def mode_conversion_adjoint(fw, i0, i1):
     gW1, gV1 = flux_grads(b1.W, b1.V, i1, abs(T) ** 2 / f0)
     gW0, gV0 = flux_grads(b0.W, b0.V, i0, -abs(T) ** 2 * f1 / f0 ** 2)
     return L, gS, gW0, gV0, gW1, gV1
+
+
+def segments_block_adjoints_checkpointed(sampler, cuts, gS_of, every):
+    """The reverse pass of segments_block_adjoints with the forward's
+    per-segment data kept only at checkpoints: the chain state before every
+    `every`-th segment is stored (memory ~ (K / every) chain states), and each
+    block of segments is recomputed from its checkpoint on the way back
+    (about one extra forward in total).  gS_of(fw_final) gives the final
+    blocks' adjoints.  Returns the per-segment own-basis block adjoints."""
+    cuts = list(cuts)
+    K = len(cuts) - 1
+    k0 = sampler.k0
+    P0, Q0 = sampler.sample(cuts[0])
+    b0 = O.Basis(*O.wave_equation_solve(P0, Q0))
+    P1, Q1 = sampler.sample(cuts[-1])
+    b1 = O.Basis(*O.wave_equation_solve(P1, Q1))
+    n = P0.shape[0]
+    I = np.eye(n, dtype=np.complex128)
+    Z = np.zeros((n, n), np.complex128)
+
+    def run(j0, j1, S, leftW, leftV, keep):
+        """Segments j0..j1-1 from chain state S (left basis leftW, leftV)."""
+        tape = []
+        for j in range(j0, j1):
+            a, b = cuts[j], cuts[j + 1]
+            Pa, Qa = (P0, Q0) if j == 0 else sampler.sample(a)
+            Pm, Qm = sampler.sample(0.5 * (a + b))
+            Pb, Qb = (P1, Q1) if j == K - 1 else sampler.sample(b)
+            bm = O.Basis(*O.wave_equation_solve(Pm, Qm))
+            seg, _ = O.perturbation_segment(Pm, Qm, bm, k0, a, b, (Pa, Pm, Pb), (Qa, Qm, Qb))
+            invW, invV = bm.solveW(leftW), bm.solveV(leftV)
+            A, B = 0.5 * (invW + invV), 0.5 * (invW - invV)
+            segp = O.project_left(seg, bm, leftW, leftV)
+            if keep:
+                tape.append(dict(seg=seg, segp=segp, ABM=(A, B, np.linalg.inv(A - seg[3] @ B)), prefix=S))
+            S = O.star_right(S, segp)
+            leftW, leftV = bm.W, bm.V
+        return S, leftW, leftV, tape
+
+    # forward: chain states at the checkpoints only
+    checkpoints = {}
+    S, lW, lV = [I.copy(), I.copy(), Z.copy(), Z.copy()], b0.W, b0.V
+    for j0 in range(0, K, every):
+        checkpoints[j0] = (S, lW, lV)
+        S, lW, lV, _ = run(j0, min(j0 + every, K), S, lW, lV, keep=False)
+    Sc = S
+    Ar = 0.5 * (np.linalg.solve(lW, b1.W) + np.linalg.solve(lV, b1.V))
+    Br = 0.5 * (np.linalg.solve(lW, b1.W) - np.linalg.solve(lV, b1.V))
+    Sf = O.project_right(Sc, lW, lV, b1.W, b1.V)
+    fw_final = dict(Sc=Sc, S=Sf, ABr=(Ar, Br, np.linalg.inv(Ar - Sc[2] @ Br)), b0=b0, b1=b1, k0=k0)
+    G = project_right_adjoint(Sc, fw_final["ABr"], Sf, gS_of(fw_final))
+    out = [None] * K
+    for j0 in sorted(checkpoints, reverse=True):
+        S, lW, lV = checkpoints[j0]
+        _, _, _, tape = run(j0, min(j0 + every, K), S, lW, lV, keep=True)
+        for jj in range(len(tape) - 1, -1, -1):
+            t = tape[jj]
+            G, gsegp = star_adjoint(t["prefix"], t["segp"], G)
+            out[j0 + jj] = project_left_adjoint(t["seg"], t["ABM"], t["segp"], gsegp)
+    return out

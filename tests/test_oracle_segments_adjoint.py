@@ -165,3 +165,20 @@ def test_mode_conversion_gradient_pml_waveguide(k):
     wm[k] -= hf
     fd = (objective(wp) - objective(wm)) / (2 * hf)
     assert abs(g - fd) <= 1e-5 * abs(fd), (g, fd)
+
+
+def test_checkpointed_reverse_pass_equals_full_tape():
+    """Keeping only every 7th chain state and recomputing blocks on the way
+    back gives the same per-segment adjoints as the full tape."""
+    from oracle.segments_adjoint import segments_block_adjoints_checkpointed
+    d = _cell(1.05)
+    s = make_sampler(d)
+    cuts = O.tree_cuts(O.redheffer_compute(s, d["z0"], d["z1"], pe=1e-3).nodes)
+    fw = segments_forward(s, cuts)
+    _, gS = fourier_transmission_adjoint(fw, 5)
+    full = segments_block_adjoints(fw, gS)
+    ck = segments_block_adjoints_checkpointed(make_sampler(d), cuts, lambda f: fourier_transmission_adjoint(f, 5)[1], 7)
+    assert len(full) == len(ck) == len(cuts) - 1
+    for a, b in zip(full, ck):
+        for x, y in zip(a, b):
+            assert np.abs(x - y).max() <= 1e-12 * max(np.abs(x).max(), 1e-300)
