@@ -126,3 +126,29 @@ def test_pml_factors_damp_with_complex_stretch():
     assert np.all(np.isfinite(Fx)) and np.all(np.isfinite(Fy))
     c = (nx * ny) // 2
     assert Fx[c, c].imag != 0.0 and Fy[c, c].imag != 0.0
+
+
+@pytest.mark.parametrize("method", ["redheffer", "rcwa"])
+def test_z_mirror_symmetry(method):
+    """A structure symmetric under z -> L - z between identical half-spaces:
+    the up- and down-going blocks coincide in the Fourier basis (Tuu = Tdd,
+    Rdu = Rud), for varRCWA (its trisection tree and Simpson segments are
+    mirror symmetric) and for RCWA."""
+    L = 2.0
+    zs = np.linspace(0.0, L, 9)
+    w = 0.4 + 0.5 * 4.0 * zs * (L - zs) / L ** 2      # symmetric width profile
+    c = 0.75
+    x = np.array([0.0, c - 0.2, c + 0.2, 1.5])
+    eps = np.array([[2.085, 12.11, 2.085]], dtype=np.complex128)
+    s = O.VarLayerSampler(1.55, 7, 1, x, np.array([0.0, 1.0]), eps, enable_pml=False)
+    s.add_x_rule(1, lambda z: float(np.interp(z, zs, c - 0.5 * w)))
+    s.add_x_rule(2, lambda z: float(np.interp(z, zs, c + 0.5 * w)))
+    e = O.homogeneous_basis(s, 2.085)
+    if method == "redheffer":
+        S = O.redheffer_compute(s, 0.0, L, pe=1e-4, end0=e, end1=e)
+    else:
+        S = O.rcwa_compute(s, 0.0, L, 12, end0=e, end1=e)
+    F = S.fourier_blocks()
+    scale = np.linalg.norm(F["Tuu"])
+    assert np.linalg.norm(F["Tuu"] - F["Tdd"]) <= 1e-10 * scale
+    assert np.linalg.norm(F["Rdu"] - F["Rud"]) <= 1e-10 * scale
