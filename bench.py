@@ -1,25 +1,29 @@
 #!/usr/bin/env python
 """Benchmark of the batched varRCWA S-matrix solve on B200.
 
-Workload (default): a batch of config-2 pillar unit cells -- 400 nm square
-period, 532 nm, 11x11 orders (n = 242, complex128), a tapered circular
-pillar (eps 5.8) of height 600 nm with seeded base radius U[60,140] nm and
-sidewall angle U[85,90] deg, rasterised on 256x256 pixels per z-sample, on
-an SiO2 substrate (eps 2.13) under air -- each solved by adaptive varRCWA
+Workload (default, `--workload c3`): the uneven batch of config 3 -- a queue
+of 4096 pillar unit cells (400 nm square period, tapered circular pillar of
+eps 5.8 and height 600 nm on SiO2 under air, base radius U[60,140] nm,
+sidewall angle U[85,90] deg, wavelength U[450,650] nm, harmonic truncation
+drawn from {7x7, 9x9, 11x11, 13x13, 15x15}, i.e. n = 98..450 complex128,
+rasterised on 256x256 pixels per z-sample), each solved by adaptive varRCWA
 (pe = 1e-2) and reduced to per-order reflected/transmitted power for both
-polarisations.  A step is one batched call of the C-ABI on `--batch` cells.
+polarisations.  A step is one C-ABI call on the next wave of `--batch` cells
+of the queue (the whole queue does not fit a minute of timing: at ~15
+solves/s it is several minutes of work), so K steps solve K distinct waves.
 
 Metric: S-matrix solves per second (whole job, all ranks).  `value` is the
 device time of the calls (CUDA events on the engine stream); `e2e` is the
 wall time of the same C-ABI calls from host structure descriptors to host
 order powers.  Multi-GPU runs are independent replicas (one process per
-GPU, disjoint cell seeds, no collective on the data path).
+GPU, the queue sharded by cost, no collective on the data path).
 
-`--workload c4` measures the other half of the metric: forward + adjoint
-solves of config-4 freeform metagratings (600 nm period, 633 nm, 9x9 orders,
-four 150 nm layers of 64x64 permittivity pixels) -- per-order powers and the
-gradient of T(+1,0) with respect to all 16384 pixels per stack.  The default
-config-2 line carries a short run of it under "fwd_adjoint".
+Sub-lines of the default run (one GPU, outside the timed region): config 2
+(11x11 orders), and the forward + adjoint half of the metric on config-4
+freeform metagratings (600 nm period, 633 nm, four 150 nm layers of 64x64
+permittivity pixels; per-order powers and the gradient of T(+1,0) with
+respect to all 16384 pixels per stack) at 9x9 and at 15x15 orders, each
+against the same stacks solved one per call.
 
 `--impl reference` times the CPU restatement of the reference algorithm
 (the oracle) on this machine's host cores on the same workload.
@@ -47,28 +51,51 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--batch", type=int, default=None,
-                   help="cells per step per GPU (default 128; 8 for c1, whose ~6600 segments per cell are "
-                        "all held until the star reduction)")
-    p.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4"])
+                   help="cells per step per GPU (c3: 64 cells per wave; c2 / c4: 128; c1: 8, whose ~6600 "
+                        "segments per cell are all held until the star reduction)")
+    p.add_argument("--queue", type=int, default=4096, help="c3: cells in the job queue (sharded over ranks)")
+    p.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4"])
     p.add_argument("--pe", type=float, default=None, help="varRCWA tolerance (default 1e-6 for c1, else 1e-2)")
     p.add_argument("--npix", type=int, default=256)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--cpu-cells", type=int, default=1, help="cells in the bounded CPU sample")
+    p.add_argument("--cpu-seconds", type=float, default=90.0,
+                   help="bound on the CPU samples (rounds of one cell per host core)")
     p.add_argument("--plain-cells", type=int, default=8,
                    help="cells timed one per call (the plain per-solve form of the metric); 0 skips")
-    p.add_argument("--no-adjoint", action="store_true", help="skip the fwd_adjoint sub-measurement of the c2 line")
+    p.add_argument("--no-sub", action="store_true", help="skip the c2 and forward+adjoint sub-lines")
     p.add_argument("--orders", type=int, default=9, help="c4: harmonics per axis (9 = config 4, 15 = 15x15 orders)")
     a = p.parse_args()
     if a.pe is None:
         a.pe = 1e-6 if a.workload == "c1" else 1e-2
     if a.batch is None:
-        a.batch = 8 if a.workload == "c1" else 128
+        a.batch = {"c1": 8, "c3": 64}.get(a.workload, 128)
     return a
 
 
 def make_cells(workload, batch, rank, npix, step_seed=0, orders=9):
     from varrcwa_b200.replicas import make_cells as mc
     return mc(workload, batch, rank, npix, step_seed, orders)
+
+
+class Waves:
+    """The cells of each step.  c3: consecutive waves of `batch` cells of this
+    rank's cost-balanced share of the job queue (wrapping around); other
+    workloads: the same seeded batch every step."""
+
+    def __init__(self, a, rank, world):
+        self.batch = a.batch
+        if a.workload == "c3":
+            from varrcwa_b200.replicas import rank_queue
+            self.queue = rank_queue("c3", max(a.queue, a.batch * world), rank, world, a.npix)
+        else:
+            self.queue = make_cells(a.workload, a.batch, rank, a.npix, orders=a.orders)
+        self.k = 0
+
+    def next(self):
+        q, b = self.queue, self.batch
+        out = [q[(self.k * b + i) % len(q)] for i in range(b)]
+        self.k += 1
+        return out
 
 
 # ---------------------------------------------------------------------------
@@ -168,6 +195,8 @@ def _oracle_cell(args):
     s = make_sampler(desc)
     e0, e1 = end_bases(desc, s)
     S = O.redheffer_compute(s, desc["z0"], desc["z1"], pe=pe, end0=e0, end1=e1)
+    if desc.get("end1") is None:  # config 1: the S-matrix itself is the output
+        return float(abs(S.Tuu).sum())
     R, T = O.order_powers(S, s, desc["end1"], desc["end0"], 1.0, 0.0, side="top")
     return float(R.sum() + T.sum())
 
@@ -186,52 +215,54 @@ def _oracle_stack(desc):
     return float(T.sum() + sum(float(x.sum()) for x in g))
 
 
-def cpu_sample(descs, pe):
-    """Time the oracle on the given cells with all host threads (BLAS)."""
-    t0 = time.perf_counter()
-    for d in descs:
-        if "layers" in d:
-            _oracle_stack(d)
-        else:
-            _oracle_cell((d, pe))
-    return time.perf_counter() - t0
+def _oracle_task(args):
+    desc, pe = args
+    return _oracle_stack(desc) if "layers" in desc else _oracle_cell((desc, pe))
 
 
-def run_reference(a, rank, world):
+def cpu_rounds(cells, pe, seconds, warm=None):
+    """The oracle on the host cores, one cell per process (spawn pool,
+    single-threaded BLAS): rounds of one cell per core, taken in queue order,
+    until `seconds` have elapsed (at least one round).  Returns (cells solved,
+    seconds, rounds, processes)."""
     import multiprocessing as mp
-    if world > 1 and rank != 0:
-        return  # rank 0 alone times the CPU reference
-    ncores = os.cpu_count() or 1
-    workers = max(1, ncores)
-    descs = make_cells(a.workload, workers, rank, a.npix, orders=a.orders)
     os.environ["OPENBLAS_NUM_THREADS"] = "1"
     os.environ["OMP_NUM_THREADS"] = "1"
     os.environ["MKL_NUM_THREADS"] = "1"
-    ctxm = mp.get_context("spawn")
-    with ctxm.Pool(workers) as pool:
-        if a.workload == "c4":
-            pool.map(_oracle_stack, descs[:workers])  # warm-up: imports, first BLAS call
-            t0 = time.perf_counter()
-            for _ in range(a.steps):
-                pool.map(_oracle_stack, descs)
-            dt = time.perf_counter() - t0
-        else:
-            # warm-up: one small task per worker (imports, first BLAS call)
-            for _ in range(a.warmup):
-                pool.map(_oracle_cell, [(d, 0.5) for d in make_cells(a.workload, workers, rank, 16)])
-            t0 = time.perf_counter()
-            for _ in range(a.steps):
-                pool.map(_oracle_cell, [(d, a.pe) for d in descs])
-            dt = time.perf_counter() - t0
-    value = a.steps * len(descs) / dt
+    workers = max(1, os.cpu_count() or 1)
+    done, rounds = 0, 0
+    with mp.get_context("spawn").Pool(workers) as pool:
+        if warm:  # imports and the first BLAS call in every worker
+            pool.map(_oracle_task, [(d, 0.5) for d in warm][:workers] * max(1, workers // max(1, len(warm))))
+        t0 = time.perf_counter()
+        while True:
+            chunk = [cells[(rounds * workers + i) % len(cells)] for i in range(workers)]
+            pool.map(_oracle_task, [(d, pe) for d in chunk])
+            done += len(chunk)
+            rounds += 1
+            if time.perf_counter() - t0 >= seconds:
+                break
+        dt = time.perf_counter() - t0
+    return done, dt, rounds, workers
+
+
+def run_reference(a, rank, world):
+    if world > 1 and rank != 0:
+        return  # rank 0 alone times the CPU reference
+    waves = Waves(a, 0, 1)
+    warm = make_cells("c2", 4, 0, 16) if a.workload != "c4" else None
+    # a bounded sample: as many rounds as fit the step budget of K steps
+    done, dt, rounds, workers = cpu_rounds(waves.queue, a.pe, seconds=a.cpu_seconds + 30.0, warm=warm)
+    value = done / dt
+    sample = (f"{done} cells of the same queue in {rounds} round(s) of one cell per process ({workers} spawned "
+              f"processes, single-threaded BLAS), {dt:.1f} s")
     line = {
         "impl": "reference", "metric": metric_name(a.workload), "value": value, "unit": unit_name(a.workload),
-        "n_gpus": a.gpus,
-        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * dt / a.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "complex128", "data": "synthetic",
-        "config": workload_config(a, len(descs)),
+        "n_gpus": a.gpus, "steps": rounds, "warmup": 1 if warm else 0, "ms_per_step": 1e3 * dt / rounds,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
+        "data": "synthetic", "config": workload_config(a, a.batch),
         "cpu_baseline": {"value": value, "unit": unit_name(a.workload), "cores": workers, "kind": "port",
-                         "sample": f"{len(descs)} cells per step, one per process (spawn), single-threaded BLAS"},
+                         "sample": sample},
         "e2e": {"value": value, "unit": unit_name(a.workload), "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -280,21 +311,52 @@ def workload_config(a, batch):
                 "l2": "per-step working set (GBs of matrices) exceeds the 126 MB L2; no flush needed"}
     names = {"c1": "config-1 2D taper (41 orders, n=82, TE+TM), seeded wavelengths 1.50-1.60 um",
              "c2": "config-2 pillar cells (11x11 orders, n=242, 256x256 raster)",
-             "c3": "config-3 uneven pillar batch (7..15 orders, n=98..450)"}
-    n = {"c1": 82, "c2": 242}.get(a.workload)
-    return {"workload": names[a.workload], "batch_per_gpu": batch, "n": n, "pe": a.pe,
-            "raster": f"{a.npix}x{a.npix}" if a.workload != "c1" else "2 moving core edges",
-            "integrator": "adaptive varRCWA (trisection), Redheffer star products",
-            "output": ("the full S-matrix blocks and end bases" if a.workload == "c1" else
-                       "per-order R/T, 2 polarisations, incidence from the superstrate"),
-            "l2": "per-step working set (GBs of matrices) exceeds the 126 MB L2; no flush needed"}
+             "c3": (f"config-3 uneven pillar batch: a queue of {a.queue} cells (orders uniform from 7x7..15x15, "
+                    f"n=98..450, lambda U[450,650] nm, 256x256 raster), one wave of {batch} cells per step")}
+    n = {"c1": 82, "c2": 242, "c3": "98..450"}.get(a.workload)
+    cfg = {"workload": names[a.workload], "batch_per_gpu": batch, "n": n, "pe": a.pe,
+           "raster": f"{a.npix}x{a.npix}" if a.workload != "c1" else "2 moving core edges",
+           "integrator": "adaptive varRCWA (trisection), Redheffer star products",
+           "output": ("the full S-matrix blocks and end bases" if a.workload == "c1" else
+                      "per-order R/T, 2 polarisations, incidence from the superstrate"),
+           "l2": "per-step working set (GBs of matrices) exceeds the 126 MB L2; no flush needed"}
+    if a.workload == "c3":
+        cfg["queue"] = a.queue
+        cfg["sharding"] = "queue sharded over ranks by cost (n^3), longest first onto the least loaded rank"
+    return cfg
 
 
 # ---------------------------------------------------------------------------
 # Our arm
 # ---------------------------------------------------------------------------
-def run_ours(a, rank, world, local_rank):
+def _busy(v):
+    return v.get("busy_ms") or v["ms"]
+
+
+def breakdown_of(stats):
+    tot = sum(x["ms"] for x in stats.values()) or 1.0
+    return {k: {"ms": round(v["ms"], 3), "busy_ms": round(_busy(v), 3), "share": round(v["ms"] / tot, 4),
+                "launches": v["launches"],
+                "tflops": round(v["flops"] / (_busy(v) * 1e-3) / 1e12, 3) if v["flops"] and v["ms"] else None}
+            for k, v in sorted(stats.items(), key=lambda kv: -kv[1]["ms"])}
+
+
+def io_bytes(workload, cells):
+    """Host-to-device and device-to-host bytes of one step's C-ABI call."""
     import numpy as np
+    h2d = sum(len(np.asarray(d.get("eps", [])).tobytes()) for d in cells) + 256 * len(cells)
+    if workload == "c1":  # the S-matrix blocks and both end bases come back
+        d2h = sum(8 * (2 * d["nx"] * d["ny"]) ** 2 * 16 + 2 * 2 * d["nx"] * d["ny"] * 16 for d in cells)
+    elif workload == "c4":  # R, T of one polarisation and the pixel gradient; weights go up
+        h2d = sum(sum(np.asarray(x).nbytes for x in d["layers"]) + 8 * len(d["thick"]) + 2 * 8 * d["nx"] * d["ny"]
+                  for d in cells)
+        d2h = sum(2 * 8 * d["nx"] * d["ny"] + sum(np.asarray(x).nbytes for x in d["layers"]) for d in cells)
+    else:  # per-order R and T, both polarisations
+        d2h = sum(2 * 2 * d["nx"] * d["ny"] * 8 for d in cells)
+    return h2d, d2h
+
+
+def run_ours(a, rank, world, local_rank):
     import torch
     import torch.distributed as dist
     from varrcwa_b200.capi import Context
@@ -302,8 +364,7 @@ def run_ours(a, rank, world, local_rank):
     dev = local_rank
     torch.cuda.set_device(dev)
     ctx = Context(dev)
-    descs = make_cells(a.workload, a.batch, rank, a.npix, orders=a.orders)
-
+    waves = Waves(a, rank, world)
     solve = make_solver(ctx, a.workload, a.pe, a.batch, a.orders)
 
     def barrier():
@@ -312,29 +373,31 @@ def run_ours(a, rank, world, local_rank):
 
     fp64_peak = dgemm_peak_tflops(dev) if rank == 0 else None
     for _ in range(a.warmup):
-        solve(descs)
-    adjoint = None
-    if a.workload == "c2" and world == 1 and not a.no_adjoint:
-        adjoint = measure_fwd_adjoint(ctx, rank, a.no_cpu_baseline)
+        solve(waves.next())
     ctx.set_profiling(True)
     clocks = ClockSampler(dev)
     barrier()
     torch.cuda.synchronize()
     clocks.start()
-    dev_ms = 0.0
-    launches = 0
-    t0 = time.perf_counter()
+    dev_ms, wall, launches, h2d, d2h, nonzero = 0.0, 0.0, 0, 0, 0, 0
+    step_cells = []
     for _ in range(a.steps):
-        out, ms, nl = solve(descs)
+        cells = waves.next()  # host descriptors of the step, built outside its timed call
+        step_cells.append(cells)
+        t0 = time.perf_counter()
+        out, ms, nl = solve(cells)
+        wall += time.perf_counter() - t0
         dev_ms += ms
         launches += nl
+        bi, bo = io_bytes(a.workload, cells)
+        h2d += bi
+        d2h += bo
+        nonzero += sum(1 for o in out if o["status"])
     torch.cuda.synchronize()
-    wall = time.perf_counter() - t0
     barrier()
     clk = clocks.stop()
     stats = ctx.kernel_stats()
     ctx.set_profiling(False)
-    statuses = [o["status"] for o in out]
     # max over ranks
     if world > 1:
         from varrcwa_b200.replicas import max_over_ranks
@@ -344,75 +407,72 @@ def run_ours(a, rank, world, local_rank):
     from varrcwa_b200.replicas import job_throughput
     value = job_throughput(a.batch, a.steps, world, dev_ms * 1e-3)
     e2e = job_throughput(a.batch, a.steps, world, wall)
-    m = 121 if a.workload == "c2" else None
-    h2d = sum(len(np.asarray(d.get("eps", [])).tobytes()) for d in descs) + 256 * len(descs)
-    if a.workload == "c1":  # the S-matrix blocks and both end bases come back
-        d2h = sum(8 * (2 * d["nx"] * d["ny"]) ** 2 * 16 + 2 * 2 * d["nx"] * d["ny"] * 16 for d in descs)
-    elif a.workload == "c4":  # R, T of one polarisation and the pixel gradient; weights go up
-        h2d = sum(sum(np.asarray(x).nbytes for x in d["layers"]) + 8 * len(d["thick"]) + 2 * 8 * d["nx"] * d["ny"]
-                  for d in descs)
-        d2h = sum(2 * 8 * d["nx"] * d["ny"] + sum(np.asarray(x).nbytes for x in d["layers"]) for d in descs)
-    else:  # per-order R and T, both polarisations
-        d2h = sum(2 * 2 * d["nx"] * d["ny"] * 8 for d in descs)
     roof = roofline_of(stats, fp64_peak)
     gemm = stats.get("zgemm")
-    def _busy(v):
-        return v.get("busy_ms") or v["ms"]
-    breakdown = {k: {"ms": round(v["ms"], 3), "busy_ms": round(_busy(v), 3),
-                     "share": round(v["ms"] / sum(x["ms"] for x in stats.values()), 4),
-                     "launches": v["launches"],
-                     "tflops": round(v["flops"] / (_busy(v) * 1e-3) / 1e12, 3) if v["flops"] and v["ms"] else None}
-                 for k, v in sorted(stats.items(), key=lambda kv: -kv[1]["ms"])}
     unit = unit_name(a.workload)
     line = {
         "metric": metric_name(a.workload), "value": value, "unit": unit, "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": dev_ms / a.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "complex128", "data": "synthetic",
         "config": workload_config(a, a.batch), "parallelism": f"replicas x{world}",
-        "e2e": {"value": e2e, "unit": unit, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": launches, "roofline": roof, "clocks": clk, "kernel_breakdown": breakdown,
-        "statuses_nonzero": int(sum(1 for s in statuses if s)),
+        "e2e": {"value": e2e, "unit": unit, "h2d_bytes_per_step": h2d // a.steps, "d2h_bytes_per_step": d2h // a.steps},
+        "gpu_launches": launches, "roofline": roof, "clocks": clk, "kernel_breakdown": breakdown_of(stats),
+        "statuses_nonzero": nonzero,
     }
+    if a.workload == "c3":
+        from collections import Counter
+        line["config"]["truncations_timed"] = dict(sorted(Counter(
+            f"{d['nx']}x{d['ny']}" for cells in step_cells for d in cells).items()))
     if gemm:
         line["zgemm_tflops"] = gemm["flops"] / (_busy(gemm) * 1e-3) / 1e12
         line["fp64_dgemm_peak_tflops"] = fp64_peak
     # the plain form the metric compares against: the same cells submitted
     # one structure per call on the same GPU (outside the timed region)
     if world == 1 and a.plain_cells > 0:
+        cells = step_cells[0][: a.plain_cells]
         torch.cuda.synchronize()
         tp = time.perf_counter()
-        for d in descs[: a.plain_cells]:
+        for d in cells:
             solve([d])
         torch.cuda.synchronize()
         tpl = time.perf_counter() - tp
-        plain = min(a.plain_cells, len(descs)) / tpl
-        line["plain_per_solve"] = {"value": plain, "unit": unit, "cells": min(a.plain_cells, len(descs)),
+        t0 = time.perf_counter()
+        solve(cells)  # the same cells in one call, for a like-for-like ratio
+        tb = time.perf_counter() - t0
+        line["plain_per_solve"] = {"value": len(cells) / tpl, "unit": unit, "cells": len(cells),
                                    "form": "one cell per C-ABI call, same GPU, host buffers"}
-        line["batched_over_plain"] = e2e / plain
-    if world == 1 and not a.no_cpu_baseline:
-        sample = descs[: a.cpu_cells]
-        dt = cpu_sample(sample, a.pe)
-        line["cpu_baseline"] = {"value": len(sample) / dt, "unit": unit, "cores": os.cpu_count(),
-                                "kind": "port",
-                                "sample": f"{len(sample)} cell(s) of the same workload through the numpy oracle "
-                                          f"(OpenBLAS threads = host cores), {dt:.1f} s"}
+        line["batched_over_plain"] = e2e / (len(cells) / tpl)
+        line["same_cells_batched_over_plain"] = tpl / tb
     if world == 1 and os.environ.get("VRC_LANES") is None:
         # the same step on one engine, after the timed region: the kernels'
         # uncontended rates (in the timed region the call's cells run on
         # concurrent engines, whose launches share the GPU)
         os.environ["VRC_LANES"] = "1"
         try:
-            solve(descs)  # one engine now holds all cells: let its pools grow first
+            solve(step_cells[0])  # one engine now holds all cells: let its pools grow first
             ctx.set_profiling(True)
-            solve(descs)
+            solve(step_cells[0])
             line["roofline_single_lane"] = roofline_of(ctx.kernel_stats(), fp64_peak)
-            line["roofline_single_lane"]["note"] = ("an extra step with the cells on one engine, outside the "
-                                                    "timed region")
+            line["roofline_single_lane"]["note"] = ("the first timed wave again with the cells on one engine, "
+                                                    "outside the timed region")
             ctx.set_profiling(False)
         finally:
             del os.environ["VRC_LANES"]
-    if adjoint is not None:
-        line["fwd_adjoint"] = adjoint
+    if world == 1 and not a.no_sub:
+        subs = {}
+        if a.workload != "c2":
+            subs["c2"] = measure_forward(ctx, "c2", a.pe, batch=64, steps=3)
+        if a.workload != "c4":
+            subs["fwd_adjoint"] = measure_fwd_adjoint(ctx, 9, batch=128, steps=10, plain=32)
+            subs["fwd_adjoint_15x15"] = measure_fwd_adjoint(ctx, 15, batch=32, steps=10, plain=32)
+        line.update(subs)
+    if world == 1 and not a.no_cpu_baseline:
+        done, dt, rounds, workers = cpu_rounds(waves.queue, a.pe, seconds=a.cpu_seconds,
+                                               warm=make_cells("c2", 4, 0, 16) if a.workload != "c4" else None)
+        line["cpu_baseline"] = {"value": done / dt, "unit": unit, "cores": workers, "kind": "port",
+                                "sample": f"{done} cells of the same queue through the numpy oracle, one per "
+                                          f"process ({workers} spawned, single-threaded BLAS), {rounds} round(s), "
+                                          f"{dt:.1f} s"}
     print(json.dumps(line), flush=True)
 
 
@@ -484,41 +544,56 @@ def make_solver(ctx, workload, pe, batch, orders=9):
     return solve
 
 
-def measure_fwd_adjoint(ctx, rank, no_cpu, batch=128, steps=3, warmup=3, plain=4):
-    """Short config-4 forward+adjoint measurement for the default line."""
+def measure_forward(ctx, workload, pe, batch, steps, warmup=1):
+    """A short forward sub-line (device and end-to-end solves/s)."""
     import torch
-    cells = make_cells("c4", batch, rank, 64)
-    solve = make_solver(ctx, "c4", None, batch)
+    cells = make_cells(workload, batch, 0, 256)
+    solve = make_solver(ctx, workload, pe, batch)
     for _ in range(warmup):
         solve(cells)
     torch.cuda.synchronize()
-    dev_ms = 0.0
-    launches = 0
+    dev_ms, t0 = 0.0, time.perf_counter()
+    for _ in range(steps):
+        dev_ms += solve(cells)[1]
+    wall = time.perf_counter() - t0
+    return {"metric": metric_name(workload), "value": batch * steps / (dev_ms * 1e-3), "unit": "solves/s",
+            "e2e": {"value": batch * steps / wall, "unit": "solves/s"}, "steps": steps, "warmup": warmup,
+            "config": {"workload": "config-2 pillar cells (11x11 orders, n=242, 256x256 raster)",
+                       "batch_per_gpu": batch, "pe": pe}}
+
+
+def measure_fwd_adjoint(ctx, orders, batch, steps, plain, warmup=2):
+    """Config-4 forward + adjoint: batched stacks against the same stacks one
+    forward + backward pair per call (the plain form)."""
+    import torch
+    cells = make_cells("c4", batch, 0, 64, orders=orders)
+    solve = make_solver(ctx, "c4", None, batch, orders)
+    for _ in range(warmup):
+        solve(cells)
+    torch.cuda.synchronize()
+    dev_ms, launches = 0.0, 0
     t0 = time.perf_counter()
     for _ in range(steps):
         _, ms, nl = solve(cells)
         dev_ms += ms
         launches += nl
     wall = time.perf_counter() - t0
+    solve(cells[:1])  # warm the one-stack shapes
+    torch.cuda.synchronize()
+    pc = [cells[i % len(cells)] for i in range(plain)]
     tp = time.perf_counter()
-    for d in cells[:plain]:
+    for d in pc:
         solve([d])
     tpl = time.perf_counter() - tp
-    out = {"metric": metric_name("c4"), "value": batch * steps / (dev_ms * 1e-3), "unit": "grads/s",
-           "e2e": {"value": batch * steps / wall, "unit": "grads/s"}, "steps": steps, "warmup": warmup,
-           "ms_per_step": dev_ms / steps, "gpu_launches": launches,
-           "config": {"workload": "config-4 freeform metagrating stacks (9x9 orders, n=162, 4 layers x 64x64 "
-                                  "pixels)", "batch_per_gpu": batch,
-                      "output": "per-order R/T and dT(+1,0)/d(eps) for all 16384 pixels"},
-           "plain_per_solve": {"value": plain / tpl, "unit": "grads/s", "cells": plain,
-                               "form": "one stack per forward+backward C-ABI pair"},
-           "batched_over_plain": (batch * steps / wall) / (plain / tpl)}
-    if not no_cpu:
-        dt = cpu_sample(cells[:1], None)
-        out["cpu_baseline"] = {"value": 1.0 / dt, "unit": "grads/s", "cores": os.cpu_count(), "kind": "port",
-                               "sample": f"1 stack, oracle forward + adjoint (OpenBLAS threads = host cores), "
-                                         f"{dt:.2f} s; central differences would need 2 x 16384 solves"}
-    return out
+    return {"metric": metric_name("c4"), "value": batch * steps / (dev_ms * 1e-3), "unit": "grads/s",
+            "e2e": {"value": batch * steps / wall, "unit": "grads/s"}, "steps": steps, "warmup": warmup,
+            "ms_per_step": dev_ms / steps, "gpu_launches": launches,
+            "config": {"workload": f"config-4 freeform metagrating stacks ({orders}x{orders} orders, "
+                                   f"n={2 * orders * orders}, 4 layers x 64x64 pixels)", "batch_per_gpu": batch,
+                       "output": "per-order R/T and dT(+1,0)/d(eps) for all 16384 pixels"},
+            "plain_per_solve": {"value": plain / tpl, "unit": "grads/s", "cells": plain,
+                                "form": "one stack per forward+backward C-ABI pair"},
+            "batched_over_plain": (batch * steps / wall) / (plain / tpl)}
 
 
 def main():
@@ -526,6 +601,19 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if "WORLD_SIZE" not in os.environ and a.gpus > 1:
+        # one process per GPU: relaunch this command under torchrun
+        import socket
+        s = socket.socket()
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+        s.close()
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={a.gpus}",
+               "--master-addr", "127.0.0.1", "--master-port", str(port), str(Path(__file__).resolve()),
+               *sys.argv[1:]]
+        sys.exit(subprocess.call(cmd))
+    if world != a.gpus:
+        sys.exit(f"bench.py: --gpus {a.gpus} but WORLD_SIZE={world}: launch one process per GPU")
     if a.impl == "reference":
         run_reference(a, rank, world)
         return

@@ -290,8 +290,9 @@ int vrc_zinv(vrc_context* ctx, int batch, int n, vrc_complex* A, int* status);
  * A (input, not modified), W (eigenvectors, unit 2-norm, largest component
  * real) and lam (eigenvalues) are DEVICE pointers, column-major complex128,
  * on the calling thread's current device; work is queued on `stream`
- * (a cudaStream_t, NULL = legacy default stream) and the call returns after
- * the stream has drained.  Scratch is a fixed area inside the library
+ * (a cudaStream_t, NULL = legacy default stream) and the call blocks the
+ * calling host thread until that stream has drained (it reads the
+ * convergence flag back); other streams and devices are not waited for.  Scratch is a fixed area inside the library
  * (about 22 MiB per device, held until exit), so n must be in
  * [2, VRC_EIG_NOALLOC_MAX_N]; larger n returns VRC_EINVAL.  All calls share
  * that area: calls that overlap on the GPU race and must be serialised by

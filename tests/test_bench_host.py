@@ -16,11 +16,29 @@ def bench():
 def test_defaults_and_helpers_present(bench, monkeypatch):
     monkeypatch.setattr(sys, "argv", ["bench.py"])
     a = bench.parse()
-    assert (a.gpus, a.impl, a.workload, a.batch) == (1, "ours", "c2", 128)
+    assert (a.gpus, a.impl, a.workload, a.batch, a.queue) == (1, "ours", "c3", 64, 4096)
     assert a.warmup >= 3
-    for name in ("ClockSampler", "measured_peaks", "dgemm_peak_tflops", "cpu_sample", "run_reference",
-                 "run_ours", "profiled_traffic", "workload_config", "metric_name", "make_cells"):
+    for name in ("ClockSampler", "measured_peaks", "dgemm_peak_tflops", "cpu_rounds", "run_reference",
+                 "run_ours", "profiled_traffic", "workload_config", "metric_name", "make_cells", "Waves"):
         assert hasattr(bench, name), name
+
+
+def test_c3_waves_walk_the_cost_sharded_queue(bench, monkeypatch):
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--queue", "40", "--batch", "8", "--npix", "16"])
+    a = bench.parse()
+    w = bench.Waves(a, 0, 1)
+    assert len(w.queue) == 40
+    first, second = w.next(), w.next()
+    assert len(first) == 8 and first[0] is w.queue[0] and second[0] is w.queue[8]
+    sizes = {d["nx"] for d in w.queue}
+    assert sizes <= {7, 9, 11, 13, 15} and len(sizes) >= 3  # uneven truncations
+    # two ranks split the queue by cost, disjointly
+    q0, q1 = bench.Waves(a, 0, 2).queue, bench.Waves(a, 1, 2).queue
+    assert len(q0) + len(q1) == 40
+    key = lambda d: (d["nx"], d["lam"], d["r0"])
+    assert not ({key(d) for d in q0} & {key(d) for d in q1})
+    cfg = bench.workload_config(a, a.batch)
+    assert "4096" not in cfg["workload"] and "40 cells" in cfg["workload"]
 
 
 def test_cells_are_seeded_and_rank_disjoint(bench):

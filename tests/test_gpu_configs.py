@@ -1,0 +1,125 @@
+"""Oracle parity at every benchmark configuration's own size (GPU).
+
+Each adaptive case runs the device's own adaptive varRCWA, then replays the
+device's segmentation tree in the oracle (the accept test is a max over
+eigenbasis entries, so trees of structures with degenerate modes depend on
+the eigensolver's basis choice) and compares the Fourier-basis S-matrix
+blocks (W1 Tuu W0^-1, ...) and, where the ends are half-spaces, the
+per-order powers, at 1e-9 relative.
+
+* config 1: the 2D taper at its full truncation (41 orders, n = 82) and
+  tolerance (pe = 1e-6) on a sub-range of its length (the reference's
+  convergence driver, src/tests/test_cpu.cpp:509-529, on the same kind of
+  structure); hundreds of segments.
+* config 3: pillar cells at the two largest truncations of the uneven batch,
+  13 x 13 (n = 338) and 15 x 15 (n = 450), on the full 256 x 256 raster.
+* config 5: the eigensolver at n = 882 (the single-CTA Hessenberg kernel
+  with 32 rows per lane, the blocked inversion with 8-column panels) against
+  LAPACK, and a 21 x 21-order PML waveguide cell (n = 882; the reference's
+  PML waveguide structure, src/tests/test_cpu.cpp:128-212) over a short
+  z-range.
+* the reference's own GDSII fixture (contour_extract.gds, driven by
+  src/tests/test_gds_cpu.cpp:131-146) at 13 x 11 harmonics over the driver's
+  whole z-range [-1.63, 1.36]: device P, Q at 1e-12 and the replayed varRCWA.
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import varrcwa_oracle as O
+from oracle.structures_adapter import end_bases, make_sampler
+from tests.conftest import fourier_blocks, relerr
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-9  # relative: S-matrix blocks and order powers
+GDS = Path(__file__).resolve().parent / "golden" / "contour_extract.gds"
+
+
+def _device_tree_cuts(ctx):
+    leaves = sorted((a, b) for (a, b, e, acc) in ctx.tree(0) if acc)
+    return [leaves[0][0]] + [b for (_, b) in leaves]
+
+
+def _replay_matches(ctx, d, pe):
+    r = ctx.redheffer([d], pe=pe)[0]
+    assert r["status"] == 0
+    cuts = _device_tree_cuts(ctx)
+    assert len(cuts) - 1 == r["N"]
+    s = make_sampler(d)
+    e0, e1 = end_bases(d, s)
+    S = O.redheffer_segments(s, d["z0"], d["z1"], cuts, end0=e0, end1=e1)
+    F, G = fourier_blocks(r), S.fourier_blocks()
+    for k in F:
+        assert relerr(F[k], G[k]) < TOL, k
+    return r, S, s
+
+
+def test_config1_full_truncation_tolerance_on_sub_range(ctx):
+    from varrcwa_b200 import structures as st
+    d = st.taper_2d()  # 41 orders, two moving core edges over 10 um
+    d["z1"] = 0.6      # the first 0.6 um of the taper
+    r, S, _ = _replay_matches(ctx, d, 1e-6)
+    assert r["n"] == 82 and r["N"] > 100
+
+
+@pytest.mark.parametrize("norders", [13, 15])
+def test_config3_largest_truncations(ctx, norders):
+    from varrcwa_b200 import structures as st
+    d = st.pillar_cell(3300 + norders, norders=norders, npix=256)
+    r, S, s = _replay_matches(ctx, d, 1e-2)
+    assert r["n"] == 2 * norders * norders
+    p = ctx.order_powers([d], method="redheffer", pe=1e-2, side=1)[0]
+    assert p["status"] == 0
+    for pol, (px, py) in enumerate(((1.0, 0.0), (0.0, 1.0))):
+        R, T = O.order_powers(S, s, d["end1"], d["end0"], px, py, side="top")
+        assert relerr(p["R"][pol], R) < TOL and relerr(p["T"][pol], T) < TOL, pol
+        assert abs(p["R"][pol].sum() + p["T"][pol].sum() - 1.0) < 1e-10  # lossless
+
+
+def test_config5_eigensolver_n882(ctx):
+    rng = np.random.default_rng(882)
+    n = 882
+    A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    lam, W = ctx.eig(A)
+    scale = np.linalg.norm(A, 2)
+    assert np.linalg.norm(A @ W - W * lam[None, :], 2) <= 1e-12 * n * scale
+    assert np.allclose(np.linalg.norm(W, axis=0), 1.0, rtol=0, atol=1e-12)
+    ref = list(np.linalg.eigvals(A))
+    worst = 0.0
+    for x in lam:
+        dist = np.abs(np.asarray(ref) - x)
+        k = int(np.argmin(dist))
+        worst = max(worst, float(dist[k]))
+        ref.pop(k)
+    assert worst <= 1e-10 * scale
+    # the inverse at n = 882 (blocked, 8-column panels)
+    Ai, st_ = ctx.zinv(A)
+    assert st_ == 0
+    assert np.linalg.norm(Ai @ A - np.eye(n), 2) <= 1e-10
+
+
+def test_config5_pml_waveguide_cell(ctx):
+    from varrcwa_b200 import structures as st
+    d = st.waveguide_pml(5000, norders=21)  # 4 x 2 um cell, PML 0.5 um, 64 control points
+    d["z1"] = 0.4                          # a short stretch of the 20 um converter
+    P, Q = ctx.sample_pq(d, [0.13])
+    s = make_sampler(d)
+    oP, oQ = s.sample(0.13)
+    assert relerr(P[0], oP) < 1e-12 and relerr(Q[0], oQ) < 1e-12
+    r, S, _ = _replay_matches(ctx, d, 1e-2)
+    assert r["n"] == 882
+
+
+def test_reference_gds_fixture_contour(ctx):
+    from varrcwa_b200 import capi
+    from varrcwa_b200 import structures as st
+    d = st.gds_planar(capi.gds_read(GDS), norders=(13, 11))
+    zs = [-1.63, -0.7, 0.0, 0.9, 1.36]
+    P, Q = ctx.sample_pq(d, zs)
+    s = make_sampler(d)
+    for k, z in enumerate(zs):
+        oP, oQ = s.sample(z)
+        assert relerr(P[k], oP) < 1e-12 and relerr(Q[k], oQ) < 1e-12, z
+    r, S, _ = _replay_matches(ctx, d, 1e-2)
+    assert r["N"] >= 2

@@ -63,3 +63,56 @@ def test_single_process_reduction_is_identity():
     assert replicas.max_over_ranks([1.0, 2.5]) == [1.0, 2.5]
     with pytest.raises(ValueError):
         replicas.cell_seeds("c2", replicas.RANK_STRIDE + 1, 0)
+
+
+def _shard_rank_main(rank, world, port, out):
+    import torch.distributed as dist
+
+    from varrcwa_b200 import replicas
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        mine = replicas.rank_queue("c3", 512, rank, world, 16)
+        cost = sum(replicas.cell_cost(d) for d in mine)
+        seeds = [(d["nx"], d["lam"], d["r0"]) for d in mine]
+        gathered = [None] * world
+        dist.all_gather_object(gathered, (cost, seeds))
+        out.put((rank, gathered))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_shard_uneven_queue_by_cost():
+    """Config-3 queue (truncations 7..15 per axis: per-cell costs differ by
+    ~100x) sharded over two ranks: disjoint, complete, and each rank's cost
+    within the LPT bound of the mean (mean + the largest cell)."""
+    import torch.multiprocessing as mp
+
+    from varrcwa_b200 import replicas
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_shard_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=120) for _ in range(2))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    gathered = res[0]
+    assert gathered == res[1]
+    queue = replicas.make_queue("c3", 512, 16)
+    costs = [replicas.cell_cost(d) for d in queue]
+    mean = sum(costs) / 2
+    all_cells = [c for (_, cells) in gathered for c in cells]
+    assert sorted(all_cells) == sorted((d["nx"], d["lam"], d["r0"]) for d in queue)
+    assert len(set(all_cells)) == len(all_cells)
+    for cost, _ in gathered:
+        assert cost <= mean + max(costs)
+    assert max(c for c, _ in gathered) / mean < 1.001
+    # dealing by position instead would leave the ranks' costs far apart
+    rr = [sum(costs[i] for i in range(r, len(costs), 2)) for r in range(2)]
+    assert max(rr) / mean > max(c for c, _ in gathered) / mean

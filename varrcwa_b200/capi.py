@@ -98,6 +98,10 @@ def lib():
         return _lib
     if not LIB_PATH.exists():
         raise RuntimeError(f"{LIB_PATH} is missing: run `python -m varrcwa_b200.build`")
+    from . import build as _build
+    if _build.CSRC.exists() and not _build.is_current():
+        raise RuntimeError(f"{LIB_PATH} was built from other sources than the tree's: "
+                           "run `python -m varrcwa_b200.build`")
     L = C.CDLL(str(LIB_PATH))
     vp = C.c_void_p
     L.vrc_create.argtypes = [C.c_int, C.POINTER(vp)]

@@ -247,7 +247,38 @@ void for_lanes(vrc_context* ctx, int G, F&& fn, Cleanup&& cleanup) {
   }
 }
 
-// Deals the cells round-robin over the lanes and runs
+// Lane of every cell of a call on G lanes.  Cells of one truncation are
+// dealt round-robin.  A call mixing truncations is dealt by cost (n^3 per
+// cell, longest first onto the least loaded lane), so that every lane carries
+// about the same arithmetic; together with each lane starting its size
+// classes at a different class (RedhefferOpts::rotate), the lanes then work
+// on different truncations at the same time instead of all on the smallest.
+std::vector<int> deal_lanes(const std::vector<vrc::CellSpec>& specs, int G) {
+  const int C = (int)specs.size();
+  std::vector<int> lane_of(C, 0);
+  bool mixed = false;
+  for (int k = 1; k < C; ++k) mixed |= specs[k].n() != specs[0].n();
+  if (!mixed) {
+    for (int k = 0; k < C; ++k) lane_of[k] = k % G;
+    return lane_of;
+  }
+  auto cost = [&](int k) {
+    const double n = specs[k].n();
+    return n * n * n;
+  };
+  std::vector<int> order(C);
+  for (int k = 0; k < C; ++k) order[k] = k;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
+  std::vector<double> load(G, 0.0);
+  for (int k : order) {
+    const int g = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    lane_of[k] = g;
+    load[g] += cost(k);
+  }
+  return lane_of;
+}
+
+// Deals the cells over the lanes (deal_lanes) and runs
 // solve(lane index, engine, cells, their indices in the call, results) on
 // every lane.  Results come back in call order with the lane that owns each
 // one (its device blocks live in that engine).
@@ -258,9 +289,11 @@ void run_lanes(vrc_context* ctx, const std::vector<vrc::CellSpec>& specs, std::v
   const int G = lane_count(C);
   std::vector<std::vector<vrc::CellSpec>> gs(G);
   std::vector<std::vector<int>> ids(G);
-  for (int c = 0; c < C; ++c) {
-    gs[c % G].push_back(specs[c]);
-    ids[c % G].push_back(c);
+  const std::vector<int> lane_of = deal_lanes(specs, G);
+  for (int c = 0; c < C; ++c) ids[lane_of[c]].push_back(c);
+  for (int g = 0; g < G; ++g) {
+    std::sort(ids[g].begin(), ids[g].end());  // call order inside a lane
+    for (int c : ids[g]) gs[g].push_back(specs[c]);
   }
   std::vector<std::vector<vrc::CellResult>> out(G);
   for_lanes(
@@ -462,8 +495,12 @@ int vrc_redheffer(vrc_context* ctx, int ncells, const vrc_cell* cells, double pe
     std::vector<int> owner;
     Timed tm(ctx);
     run_lanes(ctx, specs, res, owner,
-              [&](int, vrc::Engine& E, const std::vector<vrc::CellSpec>& sp, const std::vector<int>&,
-                  std::vector<vrc::CellResult>& r) { E.redheffer(sp, o, r); });
+              [&](int g, vrc::Engine& E, const std::vector<vrc::CellSpec>& sp, const std::vector<int>&,
+                  std::vector<vrc::CellResult>& r) {
+                vrc::Engine::RedhefferOpts lo = o;
+                lo.rotate = g;
+                E.redheffer(sp, lo, r);
+              });
     tm.done();
     export_results(ctx, res, owner, results);
   });
@@ -487,12 +524,13 @@ int vrc_redheffer_segments(vrc_context* ctx, int ncells, const vrc_cell* cells, 
     std::vector<int> owner;
     Timed tm(ctx);
     run_lanes(ctx, specs, res, owner,
-              [&](int, vrc::Engine& E, const std::vector<vrc::CellSpec>& sp, const std::vector<int>& ids,
+              [&](int g, vrc::Engine& E, const std::vector<vrc::CellSpec>& sp, const std::vector<int>& ids,
                   std::vector<vrc::CellResult>& r) {
                 std::vector<std::vector<double>> lc;
                 for (int c : ids) lc.push_back(cv[c]);
                 vrc::Engine::RedhefferOpts o;
                 o.cuts = &lc;
+                o.rotate = g;
                 E.redheffer(sp, o, r);
               });
     tm.done();
@@ -552,12 +590,13 @@ int vrc_order_powers(vrc_context* ctx, int ncells, const vrc_cell* cells, int me
     std::vector<std::vector<double>> Rv(ncells), Tv(ncells);
     Timed tm(ctx);
     run_lanes(ctx, specs, res, owner,
-              [&](int, vrc::Engine& E, const std::vector<vrc::CellSpec>& sp, const std::vector<int>& ids,
+              [&](int g, vrc::Engine& E, const std::vector<vrc::CellSpec>& sp, const std::vector<int>& ids,
                   std::vector<vrc::CellResult>& r) {
                 if (method == 0) {
                   vrc::Engine::RedhefferOpts o;
                   o.pe = pe;
                   o.max_depth = max_depth;
+                  o.rotate = g;
                   E.redheffer(sp, o, r);
                 } else if (method == 1) {
                   E.rcwa(sp, nslices, r);

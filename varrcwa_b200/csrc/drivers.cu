@@ -181,7 +181,10 @@ void Engine::redheffer(const std::vector<CellSpec>& cells, const RedhefferOpts& 
   start_results(cells, out);
   std::map<int, std::vector<int>> by_n;
   for (size_t c = 0; c < cells.size(); ++c) by_n[cells[c].n()].push_back((int)c);
-  for (auto& kv : by_n) {
+  std::vector<std::pair<int, std::vector<int>>> classes(by_n.begin(), by_n.end());
+  if (!classes.empty())
+    std::rotate(classes.begin(), classes.begin() + (size_t)std::max(0, o.rotate) % classes.size(), classes.end());
+  for (auto& kv : classes) {
     const int n = kv.first;
     const std::vector<int>& ids = kv.second;
     std::vector<CellSpec> sub;

@@ -287,25 +287,29 @@ void ensure_smem(const void* kernel, size_t bytes) {
 }
 
 namespace {
-// GEMM tile choices, shared by every engine of the process (the tuning of a
-// shape runs once, under the lock, even with several engines in flight)
+// GEMM tile choices, shared by every engine of the process and keyed by
+// device, order and operand modes.  A shape is timed outside the lock (other
+// engines keep launching meanwhile); the first result stored wins, so every
+// engine of a device uses one tile per shape.
 std::mutex g_tile_mu;
-std::map<int, int> g_tile;  // key n * 4 + opA * 2 + opB
+std::map<std::tuple<int, int, int>, int> g_tile;  // (device, n, opA * 2 + opB)
 }  // namespace
 
 int Engine::gemm_tile_cached(int n, int opA, int opB) const {
   std::lock_guard<std::mutex> lock(g_tile_mu);
-  auto it = g_tile.find(n * 4 + opA * 2 + opB);
+  auto it = g_tile.find(std::make_tuple(device_, n, opA * 2 + opB));
   return it == g_tile.end() ? 0 : it->second;
 }
 
 int Engine::gemm_tile(int n, int opA, int opB, size_t batch) {
   if (const char* e = std::getenv("VRC_GEMM_TILE")) return std::atoi(e) == 32 ? 32 : 64;
   if (n > 192) return 64;  // the 64-wide tile pads at most 25% there
-  const int key = n * 4 + opA * 2 + opB;
-  std::lock_guard<std::mutex> lock(g_tile_mu);
-  auto it = g_tile.find(key);
-  if (it != g_tile.end()) return it->second;
+  const auto key = std::make_tuple(device_, n, opA * 2 + opB);
+  {
+    std::lock_guard<std::mutex> lock(g_tile_mu);
+    auto it = g_tile.find(key);
+    if (it != g_tile.end()) return it->second;
+  }
   if (batch < 64) return 64;  // tune on a batch that fills the GPU
   // time both tiles on zeroed scratch operands (a real call may update its
   // output in place, so it cannot be run twice)
@@ -334,8 +338,8 @@ int Engine::gemm_tile(int n, int opA, int opB, size_t batch) {
   for (auto* p : m3) free_mat(p, n);
   launches += 8;
   const int best = ms[1] < ms[0] ? 32 : 64;
-  g_tile[key] = best;
-  return best;
+  std::lock_guard<std::mutex> lock(g_tile_mu);
+  return g_tile.emplace(key, best).first->second;  // an engine that finished first keeps its choice
 }
 
 void Engine::gemm(std::vector<GemmDesc>& d, int n, cplx alpha, cplx beta, double delta, int opA, int opB) {

@@ -250,6 +250,10 @@ class Engine {
     double pe = 1e-2;
     int max_depth = 40;
     const std::vector<std::vector<double>>* cuts = nullptr;  // explicit segments (replay)
+    // cells of several truncations are solved one size class after another;
+    // the class order starts at class `rotate` (mod the class count), so that
+    // concurrent engines given the same mix work on different sizes at once
+    int rotate = 0;
   };
   void redheffer(const std::vector<CellSpec>& cells, const RedhefferOpts& o, std::vector<CellResult>& out);
   void rcwa(const std::vector<CellSpec>& cells, int N, std::vector<CellResult>& out);

@@ -17,11 +17,15 @@
 // threads on the same device) race on the scratch and must be serialised by
 // the caller.  The first call on a device looks up the scratch address
 // (cudaGetSymbolAddress); make that first call before any stream capture.
+// Every call blocks the calling host thread until `stream` has drained (it
+// reads the convergence flag back); other streams keep running.
 #include "../../include/vrc.h"
 #include "common.cuh"
 #include "kernels.h"
 
 #include <cstdio>
+#include <exception>
+#include <new>
 #include <map>
 #include <mutex>
 
@@ -99,7 +103,14 @@ extern "C" int vrc_eig_noalloc(int n, const vrc_complex* A, vrc_complex* W, vrc_
     (void)cudaGetLastError();
     return VRC_ENODEV;
   }
-  unsigned char* base = scratch_address(dev);
+  unsigned char* base = nullptr;
+  try {
+    base = scratch_address(dev);  // host map insert and mutex: may throw
+  } catch (const std::bad_alloc&) {
+    return VRC_ENOMEM;
+  } catch (const std::exception&) {
+    return VRC_EINVAL;
+  }
   if (!base) return VRC_ECUDA;
   if (vrc::schur_log_bytes(kMaxN) > kLogBytes) {
     fprintf(stderr, "vrc_eig_noalloc: rotation-log scratch too small\n");
@@ -133,5 +144,9 @@ extern "C" int vrc_eig_noalloc(int n, const vrc_complex* A, vrc_complex* W, vrc_
     return VRC_ECUDA;
   } catch (const vrc::StatusError& e) {
     return e.status;
+  } catch (const std::bad_alloc&) {
+    return VRC_ENOMEM;
+  } catch (const std::exception&) {
+    return VRC_EINVAL;
   }
 }

@@ -36,6 +36,45 @@ def make_cells(workload: str, batch: int, rank: int, npix: int, step_seed: int =
     return [st.pillar_config3(seed=s, npix=npix) for s in seeds]
 
 
+def cell_cost(desc: dict) -> float:
+    """Relative cost of one solve: n^3 (eigensolver and GEMMs per sample)
+    times the expected number of segments, which grows with the structure's
+    length in wavelengths (a pillar cell's 600 nm at ~550 nm is about one)."""
+    n = 2 * int(desc["nx"]) * int(desc["ny"])
+    if "layers" in desc:  # z-uniform stacks: one eigen-solve per layer
+        return float(n) ** 3 * len(desc["layers"])
+    length = abs(float(desc.get("z1", 0.0)) - float(desc.get("z0", 0.0)))
+    return float(n) ** 3 * max(1.0, length / float(desc["lam"]))
+
+
+def shard_by_cost(costs: Sequence[float], world: int) -> List[List[int]]:
+    """Partition cell indices over `world` ranks so that the per-rank cost
+    sums are balanced: longest first onto the least loaded rank (Graham's
+    LPT rule, whose makespan is within 4/3 of the optimum).  Each rank's
+    indices come back in queue order."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    load = [0.0] * world
+    shards: List[List[int]] = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        shards[r].append(i)
+        load[r] += costs[i]
+    return [sorted(s) for s in shards]
+
+
+def make_queue(workload: str, total: int, npix: int, orders: int = 9):
+    """The job's whole cell queue (seeds independent of the rank count)."""
+    return make_cells(workload, total, 0, npix, 0, orders)
+
+
+def rank_queue(workload: str, total: int, rank: int, world: int, npix: int, orders: int = 9):
+    """This rank's cost-balanced share of the job queue."""
+    q = make_queue(workload, total, npix, orders)
+    return [q[i] for i in shard_by_cost([cell_cost(d) for d in q], world)[rank]]
+
+
 def max_over_ranks(values: Sequence[float], device=None) -> List[float]:
     """Elementwise max of per-rank values over the default process group
     (identity without one).  device: where the reduction tensor lives (a CUDA

@@ -195,3 +195,18 @@ def planar_taper(w0=0.5, w1=1.2, length=4.0, lam=1.55, norders=(11, 5), thicknes
     return dict(kind="planar", lam=lam, nx=norders[0], ny=norders[1], pml=True, polys=[np.array(pts)],
                 shift=(0.0, 0.0, 0.0), pml_w=(0.5, 0.5, 0.5, 0.5), space=(1.0, 1.0, 0.8, 0.8),
                 thickness=thickness, eps_bg=eps_bg, eps_dev=eps_dev, z0=z0, z1=z1, end0=None, end1=None)
+
+
+def gds_planar(polys, norders=(13, 11), lam=1.55, shift=(2.3647, 0.0, 0.0), z0=-1.63, z1=1.36,
+               pml_w=(0.5, 0.5, 0.5, 0.5), space=(1.0, 1.3, 1.08, 1.0), thickness=0.22,
+               eps_bg=1.445 ** 2, eps_dev=3.48 ** 2):
+    """Planar device from GDSII polygons with the parameters of the
+    reference's GDS driver (src/tests/test_gds_cpu.cpp:131-146: 1.55 um,
+    x shift 2.3647, side PML 0.5 / 0.5 and spaces 1.0 / 1.3, the
+    GDSIISampler defaults below and above, SiO2 / Si at 1.445^2 / 3.48^2,
+    z in [-1.63, 1.36]).  The reference runs 25 x 21 harmonics (n = 1050);
+    `norders` sets the truncation here."""
+    return dict(kind="planar", lam=lam, nx=norders[0], ny=norders[1], pml=True,
+                polys=[np.asarray(p, dtype=np.float64) for p in polys], shift=tuple(shift), pml_w=tuple(pml_w),
+                space=tuple(space), thickness=thickness, eps_bg=eps_bg, eps_dev=eps_dev, z0=z0, z1=z1,
+                end0=None, end1=None)
