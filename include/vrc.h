@@ -43,20 +43,46 @@ enum vrc_status_code {
 };
 
 enum vrc_geometry_kind {
-  VRC_GEOM_GRID = 0,   /* tensor grid, fixed eps table, moving coordinates */
-  VRC_GEOM_PILLAR = 1, /* uniform raster of a circular pillar, linear radius */
-  VRC_GEOM_PIXELS = 2, /* fixed uniform pixel raster (z-invariant) */
-  VRC_GEOM_PLANAR = 3  /* planar device seen from above: layout polygons in (x, z) */
+  VRC_GEOM_GRID = 0,    /* tensor grid, fixed eps table, moving coordinates */
+  VRC_GEOM_PILLAR = 1,  /* uniform raster of a circular pillar, linear radius */
+  VRC_GEOM_PIXELS = 2,  /* fixed uniform pixel raster (z-invariant) */
+  VRC_GEOM_PLANAR = 3,  /* planar device seen from above: layout polygons in (x, z) */
+  VRC_GEOM_SAMPLER = 4  /* the caller's own sampler (callbacks below) */
 };
 
-/* Piecewise-linear z-rule for one coordinate (clamped outside [zs0, zsN]).
+/* The caller's own layer sampler: the two virtual functions of the
+ * reference's LayerSampler that the integrators call
+ * (src/core/LayerSampler.h:49-55).  Either fills P and Q (n x n,
+ * column-major complex128, n = 2*nx*ny, the layout of Eigen::MatrixXcs) at
+ * height z and returns 0, or returns nonzero on failure (the call then
+ * fails with VRC_EINVAL).
+ * vrc_sample_fn: replaces LayerSampler::sample; P and Q are host buffers
+ *   (pinned staging inside the engine, copied to the device afterwards).
+ * vrc_sample_device_fn: replaces LayerSampler::sampleOnGPU; P and Q are
+ *   device buffers on the context's device, preallocated by the engine as
+ *   the reference's integrators preallocate theirs
+ *   (src/gpu/RedhefferIntegratorGPU.cpp:17-20); `stream` (a cudaStream_t)
+ *   is the engine stream that reads them next: work queued on it needs no
+ *   further synchronisation, work on other streams must be complete on
+ *   return.
+ * The engine calls a sampler from the thread that runs its cell: cells of
+ * one call may be solved on concurrent host threads, so callbacks of
+ * different cells that share state must tolerate concurrent calls. */
+typedef int (*vrc_sample_fn)(void* user, double z, vrc_complex* P, vrc_complex* Q);
+typedef int (*vrc_sample_device_fn)(void* user, double z, vrc_complex* P, vrc_complex* Q, void* stream);
+
+/* Tabulated z-rule for one coordinate: x[index](z) through the knots
+ * (zs[k], vals[k]), zs increasing, constant beyond the end knots;
+ * piecewise-linear (interp 0) or the natural cubic spline (interp 1).
  * Replaces VarLayerSampler::addXRule/addYRule with a tabulated rule
- * (src/core/VarLayerSampler.cpp:42-50). */
+ * (src/core/VarLayerSampler.cpp:42-50).  The knot values are the geometric
+ * parameters of vrc_redheffer_backward. */
 typedef struct {
   int index;
   int nknots;
   const double* zs;
   const double* vals;
+  int interp;
 } vrc_rule;
 
 /* Optional host callback evaluating arbitrary coordinate rules: called with
@@ -109,6 +135,19 @@ typedef struct {
   double space[4];        /* left, right, bottom, top spaces between PML and device */
   double thickness;
   vrc_complex eps_background, eps_device;
+  /* VRC_GEOM_SAMPLER: a sampler object of the caller driving any integrator
+   * entry point (vrc_redheffer, vrc_redheffer_segments, vrc_rcwa,
+   * vrc_differential, vrc_order_powers, vrc_sample_pq), as a
+   * std::shared_ptr<LayerSampler> drives the reference integrators
+   * (src/core/RedhefferIntegrator.h:34-35).  Set sample or sample_device
+   * (sample_device wins when both are set); nx * ny = nDim / 2 is all the
+   * integrators need, lambda gives k0.  Half-space ends (has_end0/1) and
+   * order powers also need the true odd nx, ny and the periods Lx, Ly
+   * (periodic boundaries), from which the engine forms the half-space
+   * bases itself. */
+  vrc_sample_fn sample;
+  vrc_sample_device_fn sample_device;
+  void* sample_user;
 } vrc_cell;
 
 /* Outputs of one integration.  Matrix pointers may be NULL (not copied). */
@@ -173,6 +212,32 @@ int vrc_redheffer_segments(vrc_context* ctx, int ncells, const vrc_cell* cells, 
  * evaluation order (breadth-first).  Returns the node count (may exceed
  * max_nodes; arrays hold the first max_nodes). */
 int vrc_get_tree(vrc_context* ctx, int cell, int max_nodes, double* a, double* b, double* err, int* accepted);
+
+/* ---- gradients of adaptive cells with respect to geometric parameters ------
+ * No counterpart in the reference, which has no integrator gradients (its
+ * building block is the forward-mode dP/dx of Layer::waveEqnCoeff,
+ * src/rcwa/Layer.cpp:104-162); this pair is the C form of an autograd
+ * function.  vrc_redheffer_forward is vrc_redheffer (same arguments and
+ * results) and keeps the cells and their accepted segmentations for
+ * vrc_redheffer_backward until the next forward on the context.
+ *
+ * vrc_redheffer_backward takes, per cell in call order, the cotangents of
+ * the forward's outputs -- gS: 4 n*n (Tdd, Tuu, Rud, Rdu), gB: 4 n*n (W0,
+ * V0, W1, V1; NULL: none) -- with the convention dL = Re sum conj(g) dX, and
+ * returns grad: per cell, dL/d vals[k] of every knot of every x rule, then
+ * every y rule (sum of nknots doubles per cell).  Cells must be
+ * VRC_GEOM_GRID; a geometry callback must not overwrite ruled coordinates.
+ * The gradient is that of the forward on its accepted segmentation (bases
+ * frozen inside, end bases differentiated through their eigen step; exact
+ * for objectives that do not depend on how the end modes are normalised,
+ * e.g. Fourier-basis blocks and flux-normalised modal powers).  The reverse
+ * pass recomputes the segment chain, keeping a checkpoint every
+ * `checkpoint_every` segments (0: about the square root of the count), and
+ * recomputes each block from its checkpoint. */
+int vrc_redheffer_forward(vrc_context* ctx, int ncells, const vrc_cell* cells, double pe, int max_depth,
+                          vrc_result* results);
+int vrc_redheffer_backward(vrc_context* ctx, const vrc_complex* gS, const vrc_complex* gB, int checkpoint_every,
+                           double* grad);
 
 /* ---- A12: plain RCWA --------------------------------------------------------
  * Replaces RCWAIntegrator::compute(N) (src/core/RCWAIntegrator.cpp:20-87)

@@ -321,3 +321,132 @@ def segments_block_adjoints_checkpointed(sampler, cuts, gS_of, every):
             G, gsegp = star_adjoint(t["prefix"], t["segp"], G)
             out[j0 + jj] = project_left_adjoint(t["seg"], t["ABM"], t["segp"], gsegp)
     return out
+
+
+def node_adjoints(basis, k0, a, b, gseg):
+    """Adjoint of first_order_blocks with respect to its perturbations: for a
+    segment's own-basis block adjoints gseg = (gtdd, gtuu, grud, grdu), the
+    (dL/dP, dL/dQ) at its three Simpson nodes (a, midpoint, b), so that
+    Re <gseg, first_order_blocks(dP3, dQ3)> = sum_k Re <gP_k, dP_k> + Re <gQ_k, dQ_k>."""
+    gtdd, gtuu, grud, grdu = gseg
+    gam = basis.gam
+    dz = b - a
+    ph = np.exp(1j * 0.5 * dz / k0 * gam)
+    pf = np.exp(1j * dz / k0 * gam)
+    c = 1j * dz / (12 * k0)
+    cc = np.conj(c)
+    P2 = np.conj(ph)[:, None] * np.conj(ph)[None, :]
+    F = np.conj(pf)
+    gA = [cc * (F[:, None] * gtuu + gtdd * F[None, :]),
+          4.0 * cc * P2 * (gtuu + gtdd),
+          cc * (gtuu * F[None, :] + F[:, None] * gtdd)]
+    gB = [-cc * (F[:, None] * grud * F[None, :] + grdu),
+          -4.0 * cc * P2 * (grud + grdu),
+          -cc * (grud + F[:, None] * grdu * F[None, :])]
+    Wi, Vi = np.linalg.inv(basis.W), np.linalg.inv(basis.V)
+    out = []
+    for ga, gb in zip(gA, gB):
+        gx, gy = ga + gb, ga - gb
+        out.append((H(Wi) @ gx @ H(basis.V), H(Vi) @ gy @ H(basis.W)))
+    return out
+
+
+def eig_adjoint(P, Q, W, V, gam, gW, gV, ggam=None, eta=None):
+    """Adjoint of the eigen step W, gam, V = wave_equation_solve(P, Q)
+    (src/rcwa/WaveEquationSolver.cpp:24-37: A = P Q = W diag(gam^2) W^-1,
+    V = Q W diag(1/gam)) with respect to (P, Q), for cotangents gW, gV and
+    optionally ggam.
+
+    Eigenvector part: dW = W C with C_ij = (W^-1 dA W)_ij / (lam_j - lam_i)
+    off the diagonal.  Its diagonal (each column's scale and phase) is left
+    out, which is exact for objectives that do not depend on how the modes
+    are normalised (Fourier-basis S-matrix blocks, flux-normalised modal
+    powers).  Degenerate pairs are guarded by a Lorentzian broadening of
+    1 / (lam_j - lam_i): conj(d) / (|d|^2 + eta^2), eta = 1e-12 max|lam|
+    by default."""
+    lam = gam * gam
+    n = W.shape[0]
+    if eta is None:
+        eta = 1e-12 * float(np.abs(lam).max())
+    Wi = np.linalg.inv(W)
+    # V = Q W G^-1: cotangents of Q, W and gam
+    gQ = gV @ H(W / gam[None, :])
+    gWt = gW + H(Q) @ gV / np.conj(gam)[None, :]
+    ggam_t = -np.sum(np.conj(V) * gV, axis=0) / np.conj(gam)
+    if ggam is not None:
+        ggam_t = ggam_t + ggam
+    glam = ggam_t / np.conj(2.0 * gam)
+    M = H(W) @ gWt
+    d = lam[None, :] - lam[:, None]  # lam_j - lam_i
+    Fm = M * d / (np.abs(d) ** 2 + eta * eta)
+    Fm[np.arange(n), np.arange(n)] = glam
+    gA = H(Wi) @ Fm @ H(W)
+    gP = gA @ H(Q)
+    gQ = gQ + H(P) @ gA
+    return gP, gQ
+
+
+def rule_weights(zs, z, spline=False):
+    """d x(z) / d vals[k] of a coordinate rule through knots zs: the
+    piecewise-linear hat functions (clamped outside), or the natural cubic
+    spline's cardinal functions (the spline is linear in its values)."""
+    from .structures_adapter import _pwl, natural_spline_eval
+    ev = natural_spline_eval if spline else _pwl
+    K = len(zs)
+    return np.array([ev(zs, np.eye(K)[k], z) for k in range(K)])
+
+
+def knot_gradient(desc, cuts, gS, gW0=None, gV0=None, gW1=None, gV1=None, h=1e-6):
+    """dL/d(knot values) of every coordinate rule of a grid cell (x rules
+    first, then y rules, each rule's knots in order), for cotangents gS of the
+    final blocks and optional explicit cotangents of the end bases: the
+    algorithm of the device backward.
+
+    Per segment the own-basis block adjoints (segments_block_adjoints) are
+    turned into (dL/dP, dL/dQ) at its Simpson nodes (node_adjoints); the end
+    bases' cotangents (projections and explicit terms) into (dL/dP, dL/dQ) at
+    z0 and z1 (eig_adjoint).  At every node each moving coordinate's
+    dP/dx, dQ/dx is a central difference of the sampler (+-h on that
+    coordinate alone), contracted to dL/dx(z) and spread over the rule's knots
+    by d x(z) / d vals."""
+    from .structures_adapter import make_sampler
+    s = make_sampler(desc)
+    fw = segments_forward(s, cuts)
+    gsegs, gfirst = segments_block_adjoints(fw, gS, want_first=True)
+    spline = bool(desc.get("spline"))
+    rules = [(0, r) for r in desc.get("xrules", [])] + [(1, r) for r in desc.get("yrules", [])]
+
+    def shifted(axis, idx, dlt):
+        d = dict(desc)
+        key = "x" if axis == 0 else "y"
+        rk = "xrules" if axis == 0 else "yrules"
+        d[rk] = [(i, zs, np.asarray(v, float) + (dlt if i == idx else 0.0)) for (i, zs, v) in desc.get(rk, [])]
+        base = np.array(desc[key], dtype=float)
+        base[idx] += dlt
+        d[key] = base
+        return make_sampler(d)
+
+    pert = {(ax, r[0]): (shifted(ax, r[0], h), shifted(ax, r[0], -h)) for ax, r in rules}
+    out = [np.zeros(len(r[1])) for _, r in rules]
+
+    def contract(z, gP, gQ):
+        for q, (ax, (idx, zs, _)) in enumerate(rules):
+            sp, sm = pert[(ax, idx)]
+            Pp, Qp = sp.sample(z)
+            Pm, Qm = sm.sample(z)
+            dLdx = float(np.real(np.vdot(gP, (Pp - Pm) / (2 * h)) + np.vdot(gQ, (Qp - Qm) / (2 * h))))
+            out[q] += dLdx * rule_weights(zs, z, spline)
+
+    k0 = fw["k0"]
+    for t, g in zip(fw["tape"], gsegs):
+        a, b = t["a"], t["b"]
+        for z, (gP, gQ) in zip((a, 0.5 * (a + b), b), node_adjoints(t["basis"], k0, a, b, g)):
+            contract(z, gP, gQ)
+    if desc.get("end0") is None and desc.get("end1") is None:
+        Z = np.zeros_like(gS[0])
+        e = end_bases_adjoint(fw, gS, gfirst, *(x if x is not None else Z for x in (gW0, gW1, gV0, gV1)))
+        for z, b, (gW, gV) in ((cuts[0], fw["b0"], e[0:2]), (cuts[-1], fw["b1"], e[2:4])):
+            P, Q = s.sample(z)
+            gP, gQ = eig_adjoint(P, Q, b.W, b.V, b.gam, gW, gV)
+            contract(z, gP, gQ)
+    return out

@@ -36,10 +36,11 @@ def make_sampler(d):
     if kind == "grid":
         s = O.VarLayerSampler(d["lam"], d["nx"], d["ny"], d["x"], d["y"], d["eps"],
                               enable_pml=d["pml"])
+        ev = natural_spline_eval if d.get("spline") else _pwl
         for (i, zs, vals) in d.get("xrules", []):
-            s.add_x_rule(i, lambda z, zs=zs, vals=vals: _pwl(zs, vals, z))
+            s.add_x_rule(i, lambda z, zs=zs, vals=vals, ev=ev: ev(zs, vals, z))
         for (j, zs, vals) in d.get("yrules", []):
-            s.add_y_rule(j, lambda z, zs=zs, vals=vals: _pwl(zs, vals, z))
+            s.add_y_rule(j, lambda z, zs=zs, vals=vals, ev=ev: ev(zs, vals, z))
         return s
     if kind == "pillar":
         return O.RasterSampler(d["lam"], d["nx"], d["ny"], d["Lx"], d["Ly"],
@@ -60,3 +61,31 @@ def end_bases(d, sampler):
     e0 = None if d.get("end0") is None else O.homogeneous_basis(sampler, d["end0"])
     e1 = None if d.get("end1") is None else O.homogeneous_basis(sampler, d["end1"])
     return e0, e1
+
+
+def natural_spline_eval(zs, vals, z):
+    """Natural cubic spline through (zs, vals) at z, constant beyond the end
+    knots (the clamping of the piecewise-linear rules).  Second derivatives
+    from the tridiagonal system of the natural end conditions."""
+    zs = np.asarray(zs, dtype=np.float64)
+    vals = np.asarray(vals, dtype=np.float64)
+    if z <= zs[0]:
+        return float(vals[0])
+    if z >= zs[-1]:
+        return float(vals[-1])
+    K = len(zs)
+    h = np.diff(zs)
+    A = np.zeros((K, K))
+    r = np.zeros(K)
+    A[0, 0] = A[-1, -1] = 1.0
+    for i in range(1, K - 1):
+        A[i, i - 1] = h[i - 1]
+        A[i, i] = 2.0 * (h[i - 1] + h[i])
+        A[i, i + 1] = h[i]
+        r[i] = 6.0 * ((vals[i + 1] - vals[i]) / h[i] - (vals[i] - vals[i - 1]) / h[i - 1])
+    M2 = np.linalg.solve(A, r)
+    k = min(int(np.searchsorted(zs, z, side="right")) - 1, K - 2)
+    t = z - zs[k]
+    hk = h[k]
+    b = (vals[k + 1] - vals[k]) / hk - hk * (2.0 * M2[k] + M2[k + 1]) / 6.0
+    return float(vals[k] + b * t + 0.5 * M2[k] * t * t + (M2[k + 1] - M2[k]) / (6.0 * hk) * t ** 3)

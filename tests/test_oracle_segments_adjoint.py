@@ -182,3 +182,93 @@ def test_checkpointed_reverse_pass_equals_full_tape():
     for a, b in zip(full, ck):
         for x, y in zip(a, b):
             assert np.abs(x - y).max() <= 1e-12 * max(np.abs(x).max(), 1e-300)
+
+
+def test_node_adjoints_are_the_transpose_of_the_segment_formula():
+    from oracle.segments_adjoint import first_order_blocks, node_adjoints
+    rng = np.random.default_rng(7)
+    n = 12
+    W = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    V = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    gam = rng.uniform(0.5, 2.0, n) + 1j * rng.uniform(0.0, 0.3, n)
+    basis = O.Basis(W, V, gam)
+    dP3 = [rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)) for _ in range(3)]
+    dQ3 = [rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)) for _ in range(3)]
+    g = [rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)) for _ in range(4)]
+    k0, a, b = 4.0, 0.3, 0.45
+    lhs = sum(np.real(np.vdot(gi, di)) for gi, di in zip(g, first_order_blocks(basis, k0, a, b, dP3, dQ3)))
+    rhs = sum(np.real(np.vdot(gp, dp) + np.vdot(gq, dq))
+              for (gp, gq), dp, dq in zip(node_adjoints(basis, k0, a, b, g), dP3, dQ3))
+    assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+
+
+def test_eig_adjoint_matches_central_differences_of_a_gauge_invariant_objective():
+    """L = |(W diag(e^{i gam d}) W^-1)[k, k]|^2 + Re tr(V W^-1 C) does not
+    depend on how the eigenvectors are scaled; its (P, Q) gradient from
+    eig_adjoint against central differences."""
+    from oracle.segments_adjoint import H, eig_adjoint
+    d = _waveguide(np.array(st.waveguide_pml(5000, norders=5, ncontrol=6, length=3.0)["widths"]))
+    s = make_sampler(d)
+    P, Q = s.sample(0.7)
+    rng = np.random.default_rng(3)
+    n = P.shape[0]
+    Cm = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    dd, k = 0.37, 4
+
+    def obj(P_, Q_):
+        W, V, gam = O.wave_equation_solve(P_, Q_)
+        Wi = np.linalg.inv(W)
+        T = W @ (np.exp(1j * gam * dd)[:, None] * Wi)
+        return float(abs(T[k, k]) ** 2 + np.real(np.trace(V @ Wi @ Cm))), (W, V, gam)
+
+    L, (W, V, gam) = obj(P, Q)
+    Wi = np.linalg.inv(W)
+    X = np.exp(1j * gam * dd)
+    T = W @ (X[:, None] * Wi)
+    gT = np.zeros((n, n), np.complex128)
+    gT[k, k] = 2.0 * T[k, k]
+    # T = W X W^-1 (X = diag(e^{i gam d})), and tr(V W^-1 C)
+    gX = np.diag(H(W) @ gT @ H(Wi)).copy()
+    gWi = H(W * X[None, :]) @ gT + H(Cm @ V)  # from T and from V W^-1 C
+    gW = gT @ H(X[:, None] * Wi) - H(Wi) @ gWi @ H(Wi)
+    gV = H(Wi @ Cm)
+    ggam = np.conj(1j * dd * X) * gX  # T's explicit dependence on gam
+    gP, gQ = eig_adjoint(P, Q, W, V, gam, gW, gV, ggam=ggam)
+    for _ in range(3):
+        dP = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+        dQ = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+        h = 1e-6 * np.linalg.norm(P) / np.linalg.norm(dP)
+        fd = (obj(P + h * dP, Q + h * dQ)[0] - obj(P - h * dP, Q - h * dQ)[0]) / (2 * h)
+        ad = float(np.real(np.vdot(gP, dP) + np.vdot(gQ, dQ)))
+        assert abs(ad - fd) <= 1e-6 * max(abs(fd), 1e-3 * abs(L)), (ad, fd)
+
+
+def test_knot_gradient_matches_parameter_gradient_and_central_differences():
+    """The knot-level gradient (node adjoints, coordinate differences, the
+    analytic end-basis adjoint) chained to the widths of the converter equals
+    central differences of the objective on the same cuts."""
+    from oracle.segments_adjoint import H, knot_gradient, mode_conversion_adjoint
+    w = np.array(st.waveguide_pml(5000, norders=5, ncontrol=6, length=3.0)["widths"])
+    d = _waveguide(w)
+    s = make_sampler(d)
+    cuts = O.tree_cuts(O.redheffer_compute(s, d["z0"], d["z1"], pe=1e-4).nodes)
+    fw = segments_forward(s, cuts)
+    i0 = int(np.argmax(fw["b0"].gam.real))
+    i1 = int(np.argsort(-fw["b1"].gam.real)[1])
+    L, gS, gW0o, gV0o, gW1o, gV1o = mode_conversion_adjoint(fw, i0, i1)
+    gl, gr = knot_gradient(d, cuts, gS, gW0o, gV0o, gW1o, gV1o)
+    gw = -0.5 * gl + 0.5 * gr  # x_left = cx - w/2, x_right = cx + w/2
+
+    def objective(widths):
+        f = segments_forward(make_sampler(_waveguide(widths)), cuts)
+        j0 = int(np.argmax(np.abs(H(f["b0"].W) @ fw["b0"].W[:, i0])))
+        j1 = int(np.argmax(np.abs(H(f["b1"].W) @ fw["b1"].W[:, i1])))
+        return mode_conversion_adjoint(f, j0, j1)[0]
+
+    hf = 1e-5
+    for k in (0, 2, 5):
+        wp, wm = w.copy(), w.copy()
+        wp[k] += hf
+        wm[k] -= hf
+        fd = (objective(wp) - objective(wm)) / (2 * hf)
+        assert abs(gw[k] - fd) <= 1e-5 * max(abs(fd), 1e-3 * np.abs(gw).max()), (k, gw[k], fd)

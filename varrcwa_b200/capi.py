@@ -16,7 +16,7 @@ LIB_PATH = Path(__file__).resolve().parent / "libvrc.so"
 
 VRC_OK, VRC_EINVAL, VRC_ECUDA, VRC_ENOMEM, VRC_ESINGULAR, VRC_ENOCONV, VRC_ENONFINITE, VRC_ETIMEOUT, \
     VRC_EDEPTH, VRC_ENODEV = range(10)
-GEOM_GRID, GEOM_PILLAR, GEOM_PIXELS, GEOM_PLANAR = 0, 1, 2, 3
+GEOM_GRID, GEOM_PILLAR, GEOM_PIXELS, GEOM_PLANAR, GEOM_SAMPLER = 0, 1, 2, 3, 4
 
 # Every function declared in include/vrc.h.
 EXPORTS = [
@@ -24,7 +24,7 @@ EXPORTS = [
     "vrc_wave_solve", "vrc_eig", "vrc_redheffer", "vrc_redheffer_segments", "vrc_get_tree", "vrc_rcwa",
     "vrc_differential", "vrc_order_powers", "vrc_zgemm", "vrc_zinv", "vrc_set_profiling",
     "vrc_get_kernel_stats", "vrc_eig_noalloc", "vrc_stack_forward", "vrc_stack_backward", "vrc_gds_read",
-    "vrc_planar_section", "vrc_stack_fields",
+    "vrc_planar_section", "vrc_stack_fields", "vrc_redheffer_forward", "vrc_redheffer_backward",
 ]
 
 
@@ -34,7 +34,7 @@ class VrcComplex(C.Structure):
 
 class VrcRule(C.Structure):
     _fields_ = [("index", C.c_int), ("nknots", C.c_int), ("zs", C.POINTER(C.c_double)),
-                ("vals", C.POINTER(C.c_double))]
+                ("vals", C.POINTER(C.c_double)), ("interp", C.c_int)]
 
 
 GEOM_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double))
@@ -55,6 +55,7 @@ class VrcCell(C.Structure):
         ("npoly", C.c_int), ("poly_start", C.POINTER(C.c_int)), ("poly_xz", C.POINTER(C.c_double)),
         ("shift", C.c_double * 3), ("pml_w", C.c_double * 4), ("space", C.c_double * 4), ("thickness", C.c_double),
         ("eps_background", VrcComplex), ("eps_device", VrcComplex),
+        ("sample", C.c_void_p), ("sample_device", C.c_void_p), ("sample_user", C.c_void_p),
     ]
 
 
@@ -137,6 +138,9 @@ def lib():
     L.vrc_stack_fields.argtypes = [vp, C.c_int, C.c_int, CP, CP]
     L.vrc_gds_read.argtypes = [C.c_char_p, C.c_double, IP, IP, IP, DP, C.c_int, C.c_int]
     L.vrc_planar_section.argtypes = [C.POINTER(VrcCell), C.c_double, C.c_int, DP, DP, CP]
+    L.vrc_redheffer_forward.argtypes = [vp, C.c_int, C.POINTER(VrcCell), C.c_double, C.c_int,
+                                        C.POINTER(VrcResult)]
+    L.vrc_redheffer_backward.argtypes = [vp, CP, CP, C.c_int, DP]
     _lib = L
     return L
 
@@ -155,13 +159,19 @@ def _vc(z) -> VrcComplex:
     return VrcComplex(z.real, z.imag)
 
 
+SAMPLE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_double, C.POINTER(VrcComplex), C.POINTER(VrcComplex))
+SAMPLE_DEVICE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_double, C.POINTER(VrcComplex), C.POINTER(VrcComplex),
+                               C.c_void_p)
+
+
 class _CellPack:
     """A VrcCell plus the numpy buffers it points to (kept alive)."""
 
     def __init__(self, d: dict):
         self.keep = []
         c = VrcCell()
-        kind = {"grid": GEOM_GRID, "pillar": GEOM_PILLAR, "pixels": GEOM_PIXELS, "planar": GEOM_PLANAR}[d["kind"]]
+        kind = {"grid": GEOM_GRID, "pillar": GEOM_PILLAR, "pixels": GEOM_PIXELS, "planar": GEOM_PLANAR,
+                "sampler": GEOM_SAMPLER}[d["kind"]]
         c.kind = kind
         c.nx, c.ny = int(d["nx"]), int(d["ny"])
         c.pml = 1 if d.get("pml") else 0
@@ -172,6 +182,39 @@ class _CellPack:
             c.npx, c.npy = int(d["npx"]), int(d["npy"])
             c.eps_in, c.eps_out = _vc(d["eps_in"]), _vc(d["eps_out"])
             c.r0, c.r1 = float(d["r0"]), float(d["r1"])
+        elif kind == GEOM_SAMPLER:
+            # d["sample"](z) -> (P, Q) as n x n arrays (host callback), or
+            # d["sample_device"](z, P_ptr, Q_ptr, stream) filling device buffers
+            n = 2 * c.nx * c.ny
+            c.Lx, c.Ly = float(d.get("Lx", 0.0)), float(d.get("Ly", 0.0))
+            if d.get("sample_device") is not None:
+                fdev = d["sample_device"]
+
+                def dcb(user, z, P, Q, stream):
+                    try:
+                        return int(fdev(z, C.cast(P, C.c_void_p).value, C.cast(Q, C.c_void_p).value, stream) or 0)
+                    except Exception:  # noqa: BLE001 - reported to the engine as a failed sample
+                        return 1
+
+                f = SAMPLE_DEVICE_FN(dcb)
+                c.sample_device = C.cast(f, C.c_void_p)
+            else:
+                fhost = d["sample"]
+
+                def hcb(user, z, P, Q):
+                    try:
+                        Pm, Qm = fhost(z)
+                        for src, dst in ((Pm, P), (Qm, Q)):
+                            a = np.ctypeslib.as_array(C.cast(dst, C.POINTER(C.c_double)), shape=(n * n * 2,))
+                            # column-major: the bytes of the C-order transpose
+                            a[:] = np.ascontiguousarray(np.asarray(src, dtype=np.complex128).T).view(np.float64).ravel()
+                        return 0
+                    except Exception:  # noqa: BLE001 - reported to the engine as a failed sample
+                        return 1
+
+                f = SAMPLE_FN(hcb)
+                c.sample = C.cast(f, C.c_void_p)
+            self.keep.append(f)
         elif kind == GEOM_PLANAR:
             polys = [np.ascontiguousarray(p, dtype=np.float64).reshape(-1, 2) for p in d["polys"]]
             start = np.ascontiguousarray(np.cumsum([0] + [len(p) for p in polys]), dtype=np.int32)
@@ -205,7 +248,7 @@ class _CellPack:
                     zs = np.ascontiguousarray(zs, dtype=np.float64)
                     vals = np.ascontiguousarray(vals, dtype=np.float64)
                     self.keep += [zs, vals]
-                    arr[k] = VrcRule(int(idx), len(zs), _dptr(zs), _dptr(vals))
+                    arr[k] = VrcRule(int(idx), len(zs), _dptr(zs), _dptr(vals), 1 if d.get("spline") else 0)
                 self.keep.append(arr)
                 setattr(c, "n_" + name, len(rules))
                 setattr(c, name, C.cast(arr, C.POINTER(VrcRule)))
@@ -406,6 +449,42 @@ class Context:
         res, bufs = self._results(descs, blocks)
         self._check(self.L.vrc_redheffer(self.h, len(descs), cells, float(pe), int(max_depth), res))
         return self._unpack(res, bufs)
+
+    def redheffer_forward(self, descs: List[dict], pe: float = 1e-2, max_depth: int = 40):
+        """redheffer() that keeps the cells and segmentations for redheffer_backward."""
+        packs = [_CellPack(d) for d in descs]
+        cells = (VrcCell * len(descs))(*[p.cell for p in packs])
+        res, bufs = self._results(descs, True)
+        self._check(self.L.vrc_redheffer_forward(self.h, len(descs), cells, float(pe), int(max_depth), res))
+        self._grad_packs = packs  # geometry callbacks stay alive for the backward
+        self._grad_descs = descs
+        return self._unpack(res, bufs)
+
+    def redheffer_backward(self, gS, gB=None, every: int = 0):
+        """Gradient of the last redheffer_forward's cells with respect to their
+        rule knots.  gS: per cell (gTdd, gTuu, gRud, gRdu), gB: per cell
+        (gW0, gV0, gW1, gV1) or None (n x n arrays).  Returns per cell a list of
+        arrays, dL/d vals of each x rule then each y rule."""
+        descs = self._grad_descs
+
+        def pack(mats_per_cell):
+            return np.ascontiguousarray(np.concatenate(
+                [np.stack([np.asarray(m, dtype=np.complex128).T for m in ms]).reshape(-1) for ms in mats_per_cell]))
+
+        S = pack(gS)
+        B = pack(gB) if gB is not None else None
+        sizes = [[len(r[1]) for r in d.get("xrules", [])] + [len(r[1]) for r in d.get("yrules", [])] for d in descs]
+        g = np.zeros(sum(sum(z) for z in sizes))
+        self._check(self.L.vrc_redheffer_backward(self.h, _cptr(S), _cptr(B) if B is not None else None, int(every),
+                                                  _dptr(g)))
+        out, off = [], 0
+        for z in sizes:
+            per = []
+            for k in z:
+                per.append(g[off:off + k].copy())
+                off += k
+            out.append(per)
+        return out
 
     def redheffer_segments(self, descs: List[dict], cuts: List[Sequence[float]], blocks=True):
         packs = [_CellPack(d) for d in descs]

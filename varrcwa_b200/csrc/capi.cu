@@ -7,6 +7,7 @@
 #include <chrono>
 #include <cstring>
 #include <exception>
+#include <map>
 #include <memory>
 #include <string>
 #include <thread>
@@ -21,6 +22,10 @@ struct vrc_context {
   std::string err;
   vrc_timing timing{0.0, 0};
   std::vector<std::vector<vrc::NodeRecord>> trees;
+  // cells and accepted segmentations of the last vrc_redheffer_forward
+  std::vector<vrc::CellSpec> grad_cells;
+  std::vector<std::vector<double>> grad_cuts;
+  std::vector<std::vector<vrc::cplx>> grad_ends;  // per cell W0, V0, gam0, W1, V1, gam1 (host)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
@@ -127,17 +132,23 @@ vrc::CellSpec to_spec(const vrc_cell& c) {
     size_t ne = (size_t)(c.ncx - 1) * (c.ncy - 1);
     s.eps.resize(ne);
     for (size_t i = 0; i < ne; ++i) s.eps[i] = vrc::mk(c.eps[i].re, c.eps[i].im);
-    for (int i = 0; i < c.n_xrules; ++i) {
-      const vrc_rule& r = c.xrules[i];
-      if (r.nknots < 1 || !r.zs || !r.vals) throw vrc::StatusError(VRC_EINVAL, "invalid x rule");
-      s.xrules.push_back({r.index, std::vector<double>(r.zs, r.zs + r.nknots),
-                          std::vector<double>(r.vals, r.vals + r.nknots)});
-    }
-    for (int i = 0; i < c.n_yrules; ++i) {
-      const vrc_rule& r = c.yrules[i];
-      if (r.nknots < 1 || !r.zs || !r.vals) throw vrc::StatusError(VRC_EINVAL, "invalid y rule");
-      s.yrules.push_back({r.index, std::vector<double>(r.zs, r.zs + r.nknots),
-                          std::vector<double>(r.vals, r.vals + r.nknots)});
+    for (int axis = 0; axis < 2; ++axis) {
+      const int nr = axis == 0 ? c.n_xrules : c.n_yrules;
+      const vrc_rule* rs = axis == 0 ? c.xrules : c.yrules;
+      for (int i = 0; i < nr; ++i) {
+        const vrc_rule& r = rs[i];
+        if (r.nknots < 1 || !r.zs || !r.vals || r.interp < 0 || r.interp > 1)
+          throw vrc::StatusError(VRC_EINVAL, "invalid coordinate rule");
+        for (int k = 0; k + 1 < r.nknots; ++k)
+          if (!(r.zs[k + 1] > r.zs[k])) throw vrc::StatusError(VRC_EINVAL, "rule knots must increase");
+        vrc::PwlRule pr;
+        pr.index = r.index;
+        pr.zs.assign(r.zs, r.zs + r.nknots);
+        pr.vals.assign(r.vals, r.vals + r.nknots);
+        pr.interp = r.interp;
+        pr.prepare();
+        (axis == 0 ? s.xrules : s.yrules).push_back(std::move(pr));
+      }
     }
     if (c.geometry_fn) {
       vrc_geometry_fn fn = c.geometry_fn;
@@ -160,6 +171,29 @@ vrc::CellSpec to_spec(const vrc_cell& c) {
     s.thickness = c.thickness;
     s.eps_bg = vrc::mk(c.eps_background.re, c.eps_background.im);
     s.eps_dev = vrc::mk(c.eps_device.re, c.eps_device.im);
+  } else if (c.kind == VRC_GEOM_SAMPLER) {
+    if (!c.sample && !c.sample_device) throw vrc::StatusError(VRC_EINVAL, "sampler cell needs a sampler callback");
+    void* user = c.sample_user;
+    if (c.sample_device) {
+      vrc_sample_device_fn fn = c.sample_device;
+      s.dev_sample = [fn, user](double z, cplx* P, cplx* Q, cudaStream_t st) {
+        return fn(user, z, reinterpret_cast<vrc_complex*>(P), reinterpret_cast<vrc_complex*>(Q),
+                  static_cast<void*>(st));
+      };
+    } else {
+      vrc_sample_fn fn = c.sample;
+      s.host_sample = [fn, user](double z, cplx* P, cplx* Q) {
+        return fn(user, z, reinterpret_cast<vrc_complex*>(P), reinterpret_cast<vrc_complex*>(Q));
+      };
+    }
+    // the period (periodic half-space ends and order powers); 1 otherwise
+    const double Lx = c.Lx > 0 ? c.Lx : 1.0, Ly = c.Ly > 0 ? c.Ly : 1.0;
+    if ((c.has_end0 || c.has_end1) && !(c.Lx > 0 && c.Ly > 0))
+      throw vrc::StatusError(VRC_EINVAL, "sampler cell with half-space ends needs the periods Lx, Ly");
+    s.pml = false;
+    s.x = {0.0, Lx};
+    s.y = {0.0, Ly};
+    s.eps = {vrc::mk(1.0, 0.0)};
   } else {
     throw vrc::StatusError(VRC_EINVAL, "unknown geometry kind");
   }
@@ -310,13 +344,27 @@ void run_lanes(vrc_context* ctx, const std::vector<vrc::CellSpec>& specs, std::v
     }
 }
 
+// Copies the results to the caller's buffers; with ends, also every cell's
+// end bases (W0, V0, gam0, W1, V1, gam1) into host vectors.
 void export_results(vrc_context* ctx, std::vector<vrc::CellResult>& res, const std::vector<int>& owner,
-                    vrc_result* out) {
+                    vrc_result* out, std::vector<std::vector<cplx>>* ends = nullptr) {
   ctx->trees.clear();
+  if (ends) ends->assign(res.size(), {});
   for (size_t c = 0; c < res.size(); ++c) {
     vrc::CellResult& r = res[c];
     vrc::Engine& E = lane(ctx, owner[c]);
     const size_t nn = (size_t)r.n * r.n * 16, nv = (size_t)r.n * 16;
+    if (ends) {
+      const size_t n2 = (size_t)r.n * r.n, n1 = r.n;
+      std::vector<cplx>& e = (*ends)[c];
+      e.resize(4 * n2 + 2 * n1);
+      d2h(e.data(), r.W0, nn, E.stream());
+      d2h(e.data() + n2, r.V0, nn, E.stream());
+      d2h(e.data() + 2 * n2, r.gam0, nv, E.stream());
+      d2h(e.data() + 2 * n2 + n1, r.W1, nn, E.stream());
+      d2h(e.data() + 3 * n2 + n1, r.V1, nn, E.stream());
+      d2h(e.data() + 4 * n2 + n1, r.gam1, nv, E.stream());
+    }
     if (out) {
       vrc_result& o = out[c];
       d2h(o.Tdd, r.Tdd, nn, E.stream());
@@ -535,6 +583,90 @@ int vrc_redheffer_segments(vrc_context* ctx, int ncells, const vrc_cell* cells, 
               });
     tm.done();
     export_results(ctx, res, owner, results);
+  });
+}
+
+int vrc_redheffer_forward(vrc_context* ctx, int ncells, const vrc_cell* cells, double pe, int max_depth,
+                          vrc_result* results) {
+  if (!ctx) return VRC_EINVAL;
+  ctx->grad_cells.clear();
+  ctx->grad_cuts.clear();
+  ctx->grad_ends.clear();
+  return guarded(ctx, [&] {
+    if (!(pe > 0.0) || max_depth < 0) throw vrc::StatusError(VRC_EINVAL, "pe must be > 0 and max_depth >= 0");
+    auto specs = to_specs(ncells, cells);
+    vrc::Engine::RedhefferOpts o;
+    o.pe = pe;
+    o.max_depth = max_depth;
+    std::vector<vrc::CellResult> res;
+    std::vector<int> owner;
+    Timed tm(ctx);
+    run_lanes(ctx, specs, res, owner,
+              [&](int g, vrc::Engine& E, const std::vector<vrc::CellSpec>& sp, const std::vector<int>&,
+                  std::vector<vrc::CellResult>& r) {
+                vrc::Engine::RedhefferOpts lo = o;
+                lo.rotate = g;
+                E.redheffer(sp, lo, r);
+              });
+    tm.done();
+    export_results(ctx, res, owner, results, &ctx->grad_ends);
+    ctx->grad_cells = std::move(specs);
+    for (int c = 0; c < ncells; ++c) {
+      std::vector<std::pair<double, double>> leaves;
+      for (const auto& nd : ctx->trees[c])
+        if (nd.accepted) leaves.push_back({nd.a, nd.b});
+      std::sort(leaves.begin(), leaves.end());
+      std::vector<double> cuts = {leaves.front().first};
+      for (auto& l : leaves) cuts.push_back(l.second);
+      ctx->grad_cuts.push_back(std::move(cuts));
+    }
+  });
+}
+
+int vrc_redheffer_backward(vrc_context* ctx, const vrc_complex* gS, const vrc_complex* gB, int checkpoint_every,
+                           double* grad) {
+  return guarded(ctx, [&] {
+    if (!gS || !grad || checkpoint_every < 0) throw vrc::StatusError(VRC_EINVAL, "invalid arguments");
+    const auto& cells = ctx->grad_cells;
+    const int C = (int)cells.size();
+    if (C == 0) throw vrc::StatusError(VRC_EINVAL, "redheffer backward: no forward solve to differentiate");
+    std::vector<size_t> goff(C + 1, 0), soff(C + 1, 0);
+    for (int c = 0; c < C; ++c) {
+      size_t nk = 0;
+      for (const auto& r : cells[c].xrules) nk += r.zs.size();
+      for (const auto& r : cells[c].yrules) nk += r.zs.size();
+      goff[c + 1] = goff[c] + nk;
+      soff[c + 1] = soff[c] + 4 * (size_t)cells[c].n() * cells[c].n();
+    }
+    Timed tm(ctx);
+    const int G = lane_count(C);
+    const std::vector<int> lane_of = deal_lanes(cells, G);
+    std::vector<std::vector<double>> out(C);
+    for_lanes(
+        ctx, G,
+        [&](int g, vrc::Engine& E) {
+          std::map<int, std::vector<int>> by_n;  // one truncation per reverse pass
+          for (int c = 0; c < C; ++c)
+            if (lane_of[c] == g) by_n[cells[c].n()].push_back(c);
+          for (auto& kv : by_n) {
+            std::vector<vrc::CellSpec> sp;
+            std::vector<std::vector<double>> cu;
+            std::vector<const cplx*> gs, gb, ends;
+            for (int c : kv.second) {
+              sp.push_back(cells[c]);
+              cu.push_back(ctx->grad_cuts[c]);
+              gs.push_back(reinterpret_cast<const cplx*>(gS) + soff[c]);
+              gb.push_back(gB ? reinterpret_cast<const cplx*>(gB) + soff[c] : nullptr);
+              ends.push_back(ctx->grad_ends[c].data());
+            }
+            std::vector<std::vector<double>> gr;
+            E.cell_backward(sp, cu, gs, gb, ends, checkpoint_every, gr);
+            for (size_t k = 0; k < kv.second.size(); ++k) out[kv.second[k]] = std::move(gr[k]);
+          }
+        },
+        [](int) {});
+    for (int c = 0; c < C; ++c) std::memcpy(grad + goff[c], out[c].data(), out[c].size() * sizeof(double));
+    tm.done();
   });
 }
 

@@ -4,6 +4,9 @@
 // Eigen::MatrixXcs and of the reference GPU path, src/gpu/types.cuh:18).
 #pragma once
 
+#include <string>
+#include <utility>
+
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -103,7 +106,7 @@ struct CudaError {
 };
 struct StatusError {
   int status;
-  const char* what;
-  StatusError(int s, const char* w) : status(s), what(w) {}
+  std::string what;
+  StatusError(int s, std::string w) : status(s), what(std::move(w)) {}
 };
 }  // namespace vrc

@@ -135,6 +135,15 @@ void start_results(const std::vector<CellSpec>& cells, std::vector<CellResult>& 
 }
 
 void validate(const CellSpec& c) {
+  if (c.kind == GEOM_SAMPLER) {
+    // only n = 2 nx ny matters to the integrators (a LayerSampler exposes nDim)
+    if (c.nx < 1 || c.ny < 1 || c.n() > 1024) throw StatusError(ST_EINVAL, "sampler cell: need 2 <= n <= 1024");
+    if (!c.host_sample && !c.dev_sample) throw StatusError(ST_EINVAL, "sampler cell without a sampler callback");
+    if (!(c.lambda > 0.0)) throw StatusError(ST_EINVAL, "wavelength must be positive");
+    if ((c.has_end0 || c.has_end1) && ((c.nx % 2) == 0 || (c.ny % 2) == 0 || c.nx > 64 || c.ny > 64))
+      throw StatusError(ST_EINVAL, "half-space ends need the odd harmonic counts nx, ny of the sampler");
+    return;
+  }
   if (c.nx < 1 || c.ny < 1 || (c.nx % 2) == 0 || (c.ny % 2) == 0)
     throw StatusError(ST_EINVAL, "harmonic counts must be odd and positive");
   if (c.nx > 64 || c.ny > 64 || c.n() > 1024)

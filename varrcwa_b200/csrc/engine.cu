@@ -22,6 +22,65 @@ namespace vrc {
 // ---------------------------------------------------------------------------
 // Geometry helpers
 // ---------------------------------------------------------------------------
+// Natural cubic spline: on [z_i, z_(i+1)] (h = z_(i+1) - z_i, a = (z_(i+1) - z) / h,
+// b = 1 - a) x = a y_i + b y_(i+1) + ((a^3 - a) M_i + (b^3 - b) M_(i+1)) h^2 / 6,
+// with second derivatives M from the tridiagonal system
+// h_(i-1) M_(i-1) + 2 (h_(i-1) + h_i) M_i + h_i M_(i+1) = 6 (slope_i - slope_(i-1)),
+// M_0 = M_(K-1) = 0.  M is linear in y: M = D y, D formed column by column.
+void PwlRule::prepare() {
+  const size_t K = zs.size();
+  D.clear();
+  if (interp != 1 || K < 3) return;
+  D.assign(K * K, 0.0);
+  std::vector<double> h(K - 1), c(K), d(K), r(K);
+  for (size_t i = 0; i + 1 < K; ++i) h[i] = zs[i + 1] - zs[i];
+  for (size_t col = 0; col < K; ++col) {
+    auto y = [&](size_t i) { return i == col ? 1.0 : 0.0; };
+    // Thomas algorithm on the interior unknowns M_1 .. M_(K-2)
+    for (size_t i = 1; i + 1 < K; ++i) {
+      const double rhs = 6.0 * ((y(i + 1) - y(i)) / h[i] - (y(i) - y(i - 1)) / h[i - 1]);
+      const double diag = 2.0 * (h[i - 1] + h[i]);
+      if (i == 1) {
+        c[i] = h[i] / diag;
+        d[i] = rhs / diag;
+      } else {
+        const double m = diag - h[i - 1] * c[i - 1];
+        c[i] = h[i] / m;
+        d[i] = (rhs - h[i - 1] * d[i - 1]) / m;
+      }
+    }
+    r[0] = r[K - 1] = 0.0;
+    for (size_t i = K - 2; i >= 1; --i) {
+      r[i] = d[i] - (i + 2 < K ? c[i] * r[i + 1] : 0.0);
+      if (i == 1) break;
+    }
+    for (size_t i = 0; i < K; ++i) D[i * K + col] = r[i];
+  }
+}
+
+void PwlRule::weights(double z, std::vector<double>& w) const {
+  const size_t K = zs.size();
+  w.assign(K, 0.0);
+  if (K == 0) return;
+  if (z <= zs[0]) {
+    w[0] = 1.0;
+    return;
+  }
+  if (z >= zs[K - 1]) {
+    w[K - 1] = 1.0;
+    return;
+  }
+  const size_t hi = std::upper_bound(zs.begin(), zs.end(), z) - zs.begin(), lo = hi - 1;
+  const double h = zs[hi] - zs[lo];
+  const double b = (z - zs[lo]) / h, a = 1.0 - b;
+  w[lo] += a;
+  w[hi] += b;
+  if (interp == 1 && !D.empty()) {
+    const double ca = (a * a * a - a) * h * h / 6.0, cb = (b * b * b - b) * h * h / 6.0;
+    for (size_t k = 0; k < K; ++k) w[k] += ca * D[lo * K + k] + cb * D[hi * K + k];
+  }
+}
+
 double PwlRule::eval(double z) const {
   const size_t k = zs.size();
   if (k == 0) return 0.0;
@@ -29,6 +88,13 @@ double PwlRule::eval(double z) const {
   if (z >= zs[k - 1]) return vals[k - 1];
   size_t hi = std::upper_bound(zs.begin(), zs.end(), z) - zs.begin();
   size_t lo = hi - 1;
+  if (interp == 1 && !D.empty()) {
+    std::vector<double> w;
+    weights(z, w);
+    double x = 0.0;
+    for (size_t q = 0; q < k; ++q) x += w[q] * vals[q];
+    return x;
+  }
   double t = (z - zs[lo]) / (zs[hi] - zs[lo]);
   return (1.0 - t) * vals[lo] + t * vals[hi];
 }
@@ -36,6 +102,11 @@ double PwlRule::eval(double z) const {
 void CellSpec::geometry(double z, std::vector<double>& xo, std::vector<double>& yo) const {
   if (kind == GEOM_PLANAR) {
     planar_section(z, xo, yo, nullptr);
+    return;
+  }
+  if (kind == GEOM_SAMPLER) {  // only the period: the caller's sampler forms P, Q
+    xo = x;
+    yo = y;
     return;
   }
   if (kind == GEOM_PILLAR) {
@@ -118,6 +189,8 @@ Engine::~Engine() {
     cudaEventDestroy(p.b);
   }
   for (auto e : ev_pool_) cudaEventDestroy(e);
+  if (ext_ev_) cudaEventDestroy(ext_ev_);
+  if (ext_host_) cudaFreeHost(ext_host_);
   if (ws_) cudaFree(ws_);
   if (d_stage_) cudaFree(d_stage_);
   if (h_stage_) cudaFreeHost(h_stage_);
@@ -549,7 +622,7 @@ Engine::CellDev* Engine::prepare_cell(const CellSpec& c) {
                                {cd->Ky, cd->Kx, cd->KyKx, nullptr, nullptr, nullptr}};
     gemm(g, m, mk(1, 0), mk(0, 0), 0.0);
   }
-  if (c.kind != GEOM_PILLAR && c.kind != GEOM_PLANAR) {  // planar tables are formed per sample
+  if (c.kind != GEOM_PILLAR && c.kind != GEOM_PLANAR && c.kind != GEOM_SAMPLER) {  // planar: per sample
     cd->eps_count = c.eps.size();
     cd->eps_dev = (cplx*)bytes(cd->eps_count * 16);
     VRC_CUDA_CHECK(cudaMemcpyAsync(cd->eps_dev, c.eps.data(), cd->eps_count * 16, cudaMemcpyHostToDevice, stream_));
@@ -584,7 +657,78 @@ struct AsmKey {
 };
 }  // namespace
 
-void Engine::assemble(std::vector<SampleReq>& reqs, std::vector<int>* status) {
+// Samples of cells driven by the caller's own sampler (LayerSampler::sample
+// or sampleOnGPU of the reference, src/core/LayerSampler.h:49-55): a device
+// callback writes the engine's n x n buffers directly, in stream order; a
+// host callback fills pinned host memory, which is copied to the device
+// buffers asynchronously (the staging is reused only after the previous
+// copies have completed).
+void Engine::sample_external(const std::vector<SampleReq*>& rs) {
+  if (rs.empty()) return;
+  if (!ext_ev_) VRC_CUDA_CHECK(cudaEventCreateWithFlags(&ext_ev_, cudaEventDisableTiming));
+  VRC_CUDA_CHECK(cudaEventSynchronize(ext_ev_));  // staging free
+  size_t off = 0;
+  bool copied = false;
+  for (SampleReq* r : rs) {
+    const CellSpec& s = *r->spec;
+    const int n = s.n();
+    const size_t nn = (size_t)n * n;
+    int rc = 0;
+    if (s.dev_sample) {
+      rc = s.dev_sample(r->z, r->P, r->Q, stream_);
+    } else {
+      const size_t need = 2 * nn * sizeof(cplx);
+      if (off + need > ext_cap_) {
+        if (copied) {
+          VRC_CUDA_CHECK(cudaEventRecord(ext_ev_, stream_));
+          VRC_CUDA_CHECK(cudaEventSynchronize(ext_ev_));
+        }
+        off = 0;
+        if (need > ext_cap_) {
+          if (ext_host_) VRC_CUDA_CHECK(cudaFreeHost(ext_host_));
+          ext_host_ = nullptr;
+          ext_cap_ = std::max(need, (size_t)64 << 20);
+          VRC_CUDA_CHECK(cudaMallocHost(&ext_host_, ext_cap_));
+        }
+      }
+      cplx* hp = reinterpret_cast<cplx*>(ext_host_ + off);
+      rc = s.host_sample(r->z, hp, hp + nn);
+      if (rc == 0) {
+        VRC_CUDA_CHECK(cudaMemcpyAsync(r->P, hp, nn * sizeof(cplx), cudaMemcpyHostToDevice, stream_));
+        VRC_CUDA_CHECK(cudaMemcpyAsync(r->Q, hp + nn, nn * sizeof(cplx), cudaMemcpyHostToDevice, stream_));
+        copied = true;
+      }
+      off += need;
+    }
+    if (rc != 0)
+      throw StatusError(ST_EINVAL, "sampler callback failed (returned " + std::to_string(rc) + ") at z = " +
+                                       std::to_string(r->z));
+  }
+  VRC_CUDA_CHECK(cudaEventRecord(ext_ev_, stream_));
+}
+
+void Engine::assemble(std::vector<SampleReq>& reqs_in, std::vector<int>* status) {
+  if (reqs_in.empty()) return;
+  // caller-sampler cells first; the rest (and their half-space ends) below
+  std::vector<SampleReq*> ext;
+  std::vector<int> keep;
+  for (size_t i = 0; i < reqs_in.size(); ++i) {
+    if (reqs_in[i].spec->kind == GEOM_SAMPLER && !reqs_in[i].homogeneous) ext.push_back(&reqs_in[i]);
+    else keep.push_back((int)i);
+  }
+  sample_external(ext);
+  if (status && status->size() < reqs_in.size()) status->resize(reqs_in.size(), 0);
+  if (keep.empty()) return;
+  std::vector<SampleReq> reqs;
+  for (int i : keep) reqs.push_back(reqs_in[i]);
+  std::vector<int> sub_status;
+  assemble_grid(reqs, status ? &sub_status : nullptr);
+  if (status)
+    for (size_t q = 0; q < keep.size() && q < sub_status.size(); ++q)
+      if (sub_status[q]) (*status)[keep[q]] = sub_status[q];
+}
+
+void Engine::assemble_grid(std::vector<SampleReq>& reqs, std::vector<int>* status) {
   if (reqs.empty()) return;
   std::map<AsmKey, std::vector<int>> groups;
   for (size_t i = 0; i < reqs.size(); ++i) {

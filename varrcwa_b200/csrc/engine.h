@@ -13,12 +13,19 @@
 
 namespace vrc {
 
-enum GeomKind { GEOM_GRID = 0, GEOM_PILLAR = 1, GEOM_PIXELS = 2, GEOM_PLANAR = 3 };
+enum GeomKind { GEOM_GRID = 0, GEOM_PILLAR = 1, GEOM_PIXELS = 2, GEOM_PLANAR = 3, GEOM_SAMPLER = 4 };
 
+// Coordinate rule x_index(z) through knots (zs, vals), constant beyond the
+// end knots: piecewise-linear (interp 0) or the natural cubic spline
+// (interp 1).  Both are linear in vals; weights(z) gives d x(z) / d vals[k].
 struct PwlRule {
   int index;
   std::vector<double> zs, vals;
+  int interp = 0;
+  std::vector<double> D;  // spline: second derivatives = D vals (K x K, row-major)
+  void prepare();         // forms D for a spline rule
   double eval(double z) const;
+  void weights(double z, std::vector<double>& w) const;
 };
 
 // Geometry + optics of one structure (one "cell" of a batch).
@@ -54,6 +61,12 @@ struct CellSpec {
   // cross-section at z: x (crossings between the PML / spacer coordinates),
   // y, and optionally the (5 x (nx-1)) eps table, rows = y strips
   void planar_section(double z, std::vector<double>& x, std::vector<double>& y, std::vector<cplx>* eps) const;
+
+  // caller's sampler (the role of LayerSampler::sample / sampleOnGPU): P, Q
+  // at z as n x n column-major matrices, into host memory (host_sample) or
+  // into device buffers on the given stream (dev_sample); nonzero = failure
+  std::function<int(double, cplx*, cplx*)> host_sample;
+  std::function<int(double, cplx*, cplx*, cudaStream_t)> dev_sample;
 
   int ncx() const { return kind == GEOM_PILLAR ? npx + 1 : (int)x.size(); }
   int ncy() const { return kind == GEOM_PILLAR ? npy + 1 : (int)y.size(); }
@@ -172,6 +185,10 @@ class Engine {
     cplx* keep_fe33inv = nullptr;  // optional copy of fe33^-1 (m x m; periodic cells)
   };
   void assemble(std::vector<SampleReq>& reqs, std::vector<int>* status);
+  // samples of caller-sampler cells (GEOM_SAMPLER): the callbacks fill P, Q
+  void sample_external(const std::vector<SampleReq*>& reqs);
+  // Fourier-Toeplitz assembly of the geometry kinds the engine samples itself
+  void assemble_grid(std::vector<SampleReq>& reqs, std::vector<int>* status);
 
   struct EigReq {
     const cplx* P;
@@ -256,6 +273,17 @@ class Engine {
     int rotate = 0;
   };
   void redheffer(const std::vector<CellSpec>& cells, const RedhefferOpts& o, std::vector<CellResult>& out);
+  // Gradient with respect to the rule knots of grid cells of one truncation,
+  // on the accepted segmentation `cuts` of each: gS (4 n^2 per cell: the
+  // cotangents of Tdd, Tuu, Rud, Rdu) and gB (4 n^2 or null: of W0, V0, W1,
+  // V1), host column-major; ends (per cell W0, V0, gam0, W1, V1, gam1, host)
+  // are the forward's end bases, which the cotangents refer to.  grad[c]:
+  // dL/d vals of every x rule, then every y rule.  The chain is recomputed
+  // with a checkpoint every `every` segments (0: about the square root of
+  // the segment count).
+  void cell_backward(const std::vector<CellSpec>& cells, const std::vector<std::vector<double>>& cuts,
+                     const std::vector<const cplx*>& gS, const std::vector<const cplx*>& gB,
+                     const std::vector<const cplx*>& ends, int every, std::vector<std::vector<double>>& grad);
   void rcwa(const std::vector<CellSpec>& cells, int N, std::vector<CellResult>& out);
   void differential(const std::vector<CellSpec>& cells, int N, std::vector<CellResult>& out);
   void release_result(CellResult& r);
@@ -330,6 +358,10 @@ class Engine {
   size_t stage_cap_ = 0, stage_off_ = 0;
   void* ws_ = nullptr;
   size_t ws_cap_ = 0;
+  // pinned staging of host-sampler matrices and the event of its last copy
+  char* ext_host_ = nullptr;
+  size_t ext_cap_ = 0;
+  cudaEvent_t ext_ev_ = nullptr;
   bool profiling_ = false;
   cudaEvent_t origin_ = nullptr;
   // host-bubble diagnostic (VRC_HOST_STATS): time from a sync's return to

@@ -19,46 +19,14 @@
 // Each stage is batched over all stacks of the call.
 #include <cstring>
 
+#include "batch.h"
 #include "engine.h"
 
 namespace vrc {
 
 namespace {
 
-using Vec = std::vector<cplx*>;
-
-const cplx ONE{1.0, 0.0}, ZERO{0.0, 0.0}, MONE{-1.0, 0.0}, HALF{0.5, 0.0}, MHALF{-0.5, 0.0};
-
-// Batched GEMM helper over the stacks of a call: C = alpha op(A) op(B) (+ beta Cin).
-struct Batch {
-  Engine& e;
-  int C;
-  void mm(const Vec& Cm, const Vec& A, const Vec& B, cplx alpha = ONE, int oa = 0, int ob = 0,
-          const Vec* Cin = nullptr, cplx beta = ZERO, int n = 0, const Vec* rs = nullptr, double delta = 0.0) {
-    if (n <= 0) throw StatusError(ST_EINVAL, "stack GEMM without an order");
-    std::vector<GemmDesc> d(C);
-    for (int c = 0; c < C; ++c)
-      d[c] = {A[c], B[c], Cm[c], Cin ? (*Cin)[c] : nullptr, rs ? (*rs)[c] : nullptr, nullptr};
-    e.gemm(d, n, alpha, beta, delta, oa, ob);
-  }
-  Vec alloc(int n) {
-    Vec v(C);
-    for (auto& p : v) p = e.mat(n);
-    return v;
-  }
-  void release(Vec& v, int n) {
-    for (auto& p : v) e.free_mat(p, n);
-    v.clear();
-  }
-  void scale(const Vec& A, const Vec* rs, const Vec* cs, const Vec& out, int n) {
-    std::vector<const cplx*> a(A.begin(), A.end()), r(C, nullptr), s(C, nullptr);
-    if (rs) r.assign(rs->begin(), rs->end());
-    if (cs) s.assign(cs->begin(), cs->end());
-    Engine::Prof pr(e, "adjoint", 0.0, 32.0 * n * (double)n * C);
-    scale_batched(e.upload(a), rs ? e.upload(r) : nullptr, cs ? e.upload(s) : nullptr, e.upload(out), C, n,
-                  e.stream());
-  }
-};
+const cplx ONE = C_ONE, ZERO = C_ZERO, MONE = C_MONE, HALF = C_HALF, MHALF = C_MHALF;
 
 struct Carve {
   char* base;
