@@ -35,6 +35,7 @@
 // on how the end modes are scaled (Fourier-basis blocks, flux-normalised
 // modal powers).
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -197,14 +198,6 @@ int grid_for(size_t work, int threads) {
 // ---------------------------------------------------------------------------
 struct Bas {
   cplx *W = nullptr, *V = nullptr, *Wi = nullptr, *Vi = nullptr, *gam = nullptr;
-};
-
-struct Tape {  // one recomputed segment, everything its reverse needs
-  cplx* pre[4];   // chain before the segment (Tdd, Tuu, Rud, Rdu)
-  cplx* seg[4];   // own-basis blocks (tdd, tuu, rud, rdu)
-  cplx* segp[4];  // blocks with the left end in the previous basis
-  cplx *A, *B, *Minv;
-  Bas b;
 };
 
 struct Ckpt {  // chain state before segment j0
@@ -380,84 +373,115 @@ void Engine::cell_backward(const std::vector<CellSpec>& cells, const std::vector
       if (v) throw StatusError(v, "cell backward: singular end basis");
   }
 
-  // ---- one chain step for the cells in `act` (segment j of each) ----
+  // ---- blocks of segments ----
   struct St {
     cplx* S[4];
     cplx *lW, *lV, *Pa, *Qa;
   };
   std::vector<St> st(C);
   std::vector<Bas> last(C);  // inverses of each cell's last basis (exit projection)
-  double* derr = (double*)bytes((size_t)C * sizeof(double));
-  // Runs segment j for the cells in act from their states and advances the
-  // states.  With tp the segment's data go to the tape entries (which then
-  // hold them); without, they are dropped.
-  auto step = [&](int j, const std::vector<int>& act, std::vector<Tape>* tp) {
-    const int B = (int)act.size();
+  struct It {                // one segment of one cell inside a block
+    int j, c;
+    cplx *Pb, *Qb;  // sample at its right end
+    Bas b;          // midpoint basis
+    cplx *seg[4], *segp[4], *A, *B, *Minv, *pre[4];
+  };
+  // Segments [j0, j1) of the cells still running there, from their states.
+  // Node samples, midpoint bases, own-basis blocks and left projections do
+  // not depend on the chain, so they run batched over the whole block; then
+  // the star products in order, batched over the cells.  With keep, the
+  // items keep everything (the prefix chain included) for the reverse pass;
+  // without, they are dropped.  States advance to the block's end.
+  auto run_block = [&](int j0, int j1, bool keep, std::vector<It>& items) {
+    items.clear();
+    for (int j = j0; j < j1; ++j)
+      for (int c = 0; c < C; ++c)
+        if (j < K[c]) items.push_back(It{j, c});
+    const int NB = (int)items.size();
+    std::map<std::pair<int, int>, int> at;  // (cell, j) -> item
+    for (int i = 0; i < NB; ++i) at[{items[i].c, items[i].j}] = i;
     std::vector<std::pair<int, double>> rm, rb;
     std::vector<int> need_b;
-    for (int q = 0; q < B; ++q) {
-      const int c = act[q];
-      const double a = cuts[c][j], b = cuts[c][j + 1];
-      rm.push_back({c, 0.5 * (a + b)});
-      if (j + 1 < K[c]) {
-        rb.push_back({c, b});
-        need_b.push_back(q);
+    for (int i = 0; i < NB; ++i) {
+      const It& it = items[i];
+      const double za = cuts[it.c][it.j], zb = cuts[it.c][it.j + 1];
+      rm.push_back({it.c, 0.5 * (za + zb)});
+      if (it.j + 1 < K[it.c]) {
+        rb.push_back({it.c, zb});
+        need_b.push_back(i);
       }
     }
     Vec Pm, Qm, Pbn, Qbn;
     sample_into(rm, nullptr, Pm, Qm);
     sample_into(rb, nullptr, Pbn, Qbn);
-    Vec Pb(B), Qb(B);
-    for (int q = 0; q < B; ++q) {  // the exit sample: one more holder
-      Pb[q] = P1[act[q]];
-      Qb[q] = Q1[act[q]];
+    for (int i = 0; i < NB; ++i) {  // the exit sample: one more holder
+      items[i].Pb = P1[items[i].c];
+      items[i].Qb = Q1[items[i].c];
     }
     for (size_t k = 0; k < need_b.size(); ++k) {
-      Pb[need_b[k]] = Pbn[k];
-      Qb[need_b[k]] = Qbn[k];
+      items[need_b[k]].Pb = Pbn[k];
+      items[need_b[k]].Qb = Qbn[k];
     }
-    for (int q = 0; q < B; ++q)
-      if (Pb[q] == P1[act[q]]) {
-        hold(Pb[q]);
-        hold(Qb[q]);
+    for (auto& it : items)
+      if (it.Pb == P1[it.c]) {
+        hold(it.Pb);
+        hold(it.Qb);
       }
     std::vector<Bas> bm;
     decompose(Pm, Qm, bm);
-    Batch bt{*this, B};
-    Vec seg[4], segp[4], Sn[4];
+    for (int i = 0; i < NB; ++i) items[i].b = bm[i];
+    // left sample and basis of every item: the state's for the block's first
+    // segment, the previous item's otherwise
+    Vec Pa(NB), Qa(NB), lW(NB), lV(NB);
+    for (int i = 0; i < NB; ++i) {
+      const It& it = items[i];
+      if (it.j == j0) {
+        Pa[i] = st[it.c].Pa;
+        Qa[i] = st[it.c].Qa;
+        lW[i] = st[it.c].lW;
+        lV[i] = st[it.c].lV;
+      } else {
+        const It& pv = items[at.at({it.c, it.j - 1})];
+        Pa[i] = pv.Pb;
+        Qa[i] = pv.Qb;
+        lW[i] = pv.b.W;
+        lV[i] = pv.b.V;
+      }
+    }
+    Batch bt{*this, NB};
+    Vec seg[4], segp[4];
     for (int k = 0; k < 4; ++k) {
-      seg[k].resize(B);
-      segp[k].resize(B);
-      Sn[k].resize(B);
-      for (int q = 0; q < B; ++q) {
-        seg[k][q] = own();
-        segp[k][q] = own();
-        Sn[k][q] = own();
+      seg[k].resize(NB);
+      segp[k].resize(NB);
+      for (int i = 0; i < NB; ++i) {
+        items[i].seg[k] = seg[k][i] = own();
+        items[i].segp[k] = segp[k][i] = own();
       }
     }
     {
+      double* derr = (double*)bytes((size_t)NB * sizeof(double));
       std::vector<SegReq> sr;
-      for (int q = 0; q < B; ++q) {
-        const int c = act[q];
-        sr.push_back({Pm[q], Qm[q], bm[q].W, bm[q].V, bm[q].Wi, bm[q].Vi, bm[q].gam, st[c].Pa, st[c].Qa, Pb[q], Qb[q],
-                      cuts[c][j], cuts[c][j + 1], cells[c].k0(), seg[0][q], seg[1][q], seg[2][q], seg[3][q],
-                      derr + q});
+      for (int i = 0; i < NB; ++i) {
+        const It& it = items[i];
+        sr.push_back({Pm[i], Qm[i], it.b.W, it.b.V, it.b.Wi, it.b.Vi, it.b.gam, Pa[i], Qa[i], it.Pb, it.Qb,
+                      cuts[it.c][it.j], cuts[it.c][it.j + 1], cells[it.c].k0(), seg[0][i], seg[1][i], seg[2][i],
+                      seg[3][i], derr + i});
       }
       segments(sr, n);
+      free_bytes(derr, (size_t)NB * sizeof(double));
     }
-    // left projection with its matrices kept: A, B = (Wm^-1 lW +- Vm^-1 lV) / 2
-    Vec A(B), Bm(B), Mi(B), T1 = bt.alloc(n), T2 = bt.alloc(n);
-    for (int q = 0; q < B; ++q) {
-      A[q] = own();
-      Bm[q] = own();
-      Mi[q] = own();
+    for (int i = 0; i < NB; ++i) {
+      drop(Pm[i]);
+      drop(Qm[i]);
     }
-    Vec lW(B), lV(B), Wi(B), Vi(B);
-    for (int q = 0; q < B; ++q) {
-      lW[q] = st[act[q]].lW;
-      lV[q] = st[act[q]].lV;
-      Wi[q] = bm[q].Wi;
-      Vi[q] = bm[q].Vi;
+    // left projections with their matrices kept: A, B = (Wm^-1 lW +- Vm^-1 lV) / 2
+    Vec A(NB), Bm(NB), Mi(NB), Wi(NB), Vi(NB), T1 = bt.alloc(n), T2 = bt.alloc(n);
+    for (int i = 0; i < NB; ++i) {
+      items[i].A = A[i] = own();
+      items[i].B = Bm[i] = own();
+      items[i].Minv = Mi[i] = own();
+      Wi[i] = items[i].b.Wi;
+      Vi[i] = items[i].b.Vi;
     }
     bt.mm(T1, Wi, lW, C_ONE, 0, 0, nullptr, C_ZERO, n);
     bt.mm(T2, Vi, lV, C_ONE, 0, 0, nullptr, C_ZERO, n);
@@ -467,7 +491,10 @@ void Engine::cell_backward(const std::vector<CellSpec>& cells, const std::vector
       axpby(t1, t2, Bm, C_HALF, C_MHALF, 0.0, n);
     }
     bt.mm(Mi, seg[3], Bm, C_MONE, 0, 0, &A, C_ONE, n);  // M = A - rdu B
-    inverse(Mi, n, nullptr);
+    std::vector<int> ist;
+    inverse(Mi, n, &ist);
+    for (int v : ist)
+      if (v) throw StatusError(v, "cell backward: singular left projection");
     bt.mm(T1, seg[3], A, C_ONE, 0, 0, &Bm, C_MONE, n);  // rdu A - B
     bt.mm(segp[3], Mi, T1, C_ONE, 0, 0, nullptr, C_ZERO, n);
     bt.mm(segp[0], Mi, seg[0], C_ONE, 0, 0, nullptr, C_ZERO, n);
@@ -475,68 +502,77 @@ void Engine::cell_backward(const std::vector<CellSpec>& cells, const std::vector
     bt.mm(segp[2], T2, segp[0], C_ONE, 0, 0, &seg[2], C_ONE, n);
     bt.mm(T1, seg[1], A, C_ONE, 0, 0, nullptr, C_ZERO, n);
     bt.mm(segp[1], T2, segp[3], C_ONE, 0, 0, &T1, C_ONE, n);
-    {
-      std::vector<StarReq> sq;
-      for (int q = 0; q < B; ++q) {
-        const St& s = st[act[q]];
-        sq.push_back({s.S[0], s.S[1], s.S[2], s.S[3], segp[0][q], segp[1][q], segp[2][q], segp[3][q], Sn[0][q],
-                      Sn[1][q], Sn[2][q], Sn[3][q]});
-      }
-      star(sq, n, nullptr);
-    }
     bt.release(T1, n);
     bt.release(T2, n);
-    for (int q = 0; q < B; ++q) {
-      const int c = act[q];
-      St& s = st[c];
-      drop(Pm[q]);
-      drop(Qm[q]);
-      if (j + 1 == K[c] && !tp) {  // exit projection (first pass): the last basis's inverses
-        last[c].Wi = bm[q].Wi;
-        last[c].Vi = bm[q].Vi;
-        hold(bm[q].Wi);
-        hold(bm[q].Vi);
+    // the chain, segment by segment (batched over the cells)
+    for (int j = j0; j < j1; ++j) {
+      std::vector<StarReq> sq;
+      std::vector<int> idx;
+      for (int c = 0; c < C; ++c)
+        if (j < K[c]) idx.push_back(at.at({c, j}));
+      std::vector<std::array<cplx*, 4>> Sn(idx.size());
+      for (size_t q = 0; q < idx.size(); ++q) {
+        It& it = items[idx[q]];
+        St& s = st[it.c];
+        for (int k = 0; k < 4; ++k) Sn[q][k] = own();
+        sq.push_back({s.S[0], s.S[1], s.S[2], s.S[3], it.segp[0], it.segp[1], it.segp[2], it.segp[3], Sn[q][0],
+                      Sn[q][1], Sn[q][2], Sn[q][3]});
       }
-      if (tp) {
-        Tape& t = (*tp)[q];
+      std::vector<int> sst;
+      star(sq, n, &sst);
+      for (int v : sst)
+        if (v) throw StatusError(v, "cell backward: singular star product");
+      for (size_t q = 0; q < idx.size(); ++q) {
+        It& it = items[idx[q]];
+        St& s = st[it.c];
         for (int k = 0; k < 4; ++k) {
-          t.pre[k] = s.S[k];
-          hold(s.S[k]);
-          t.seg[k] = seg[k][q];
-          t.segp[k] = segp[k][q];
+          it.pre[k] = s.S[k];  // the item takes the state's reference
+          s.S[k] = Sn[q][k];
         }
-        t.A = A[q];
-        t.B = Bm[q];
-        t.Minv = Mi[q];
-        t.b = bm[q];
-        hold(bm[q].W);  // the tape's and the state's (left basis) holds
-        hold(bm[q].V);
-      } else {
-        for (int k = 0; k < 4; ++k) {
-          drop(seg[k][q]);
-          drop(segp[k][q]);
-        }
-        drop(A[q]);
-        drop(Bm[q]);
-        drop(Mi[q]);
-        drop(bm[q].Wi);
-        drop(bm[q].Vi);
-        free_vec(bm[q].gam, n);
       }
-      // advance the state: it drops what it held and takes the new pieces
-      for (int k = 0; k < 4; ++k) {
-        drop(s.S[k]);
-        s.S[k] = Sn[k][q];
-      }
-      drop(s.lW);
-      drop(s.lV);
-      s.lW = bm[q].W;
-      s.lV = bm[q].V;
-      drop(s.Pa);
-      drop(s.Qa);
-      s.Pa = Pb[q];
-      s.Qa = Qb[q];
     }
+    // states to the block's end: left basis and sample of each cell's last item
+    for (int c = 0; c < C; ++c) {
+      if (j0 >= K[c]) continue;
+      const It& lt = items[at.at({c, std::min(j1, K[c]) - 1})];
+      St& s = st[c];
+      for (cplx* p : {s.lW, s.lV, s.Pa, s.Qa}) drop(p);
+      s.lW = lt.b.W;
+      s.lV = lt.b.V;
+      s.Pa = lt.Pb;
+      s.Qa = lt.Qb;
+      for (cplx* p : {s.lW, s.lV, s.Pa, s.Qa}) hold(p);
+      if (!keep && lt.j + 1 == K[c]) {  // exit projection (first pass): the last basis's inverses
+        last[c].Wi = lt.b.Wi;
+        last[c].Vi = lt.b.Vi;
+        hold(last[c].Wi);
+        hold(last[c].Vi);
+      }
+    }
+    if (!keep) {
+      for (It& it : items) {
+        for (int k = 0; k < 4; ++k) {
+          drop(it.seg[k]);
+          drop(it.segp[k]);
+          drop(it.pre[k]);
+        }
+        for (cplx* p : {it.A, it.B, it.Minv, it.b.W, it.b.V, it.b.Wi, it.b.Vi, it.Pb, it.Qb}) drop(p);
+        free_vec(it.b.gam, n);
+      }
+      items.clear();
+    }
+  };
+  auto release_items = [&](std::vector<It>& items) {
+    for (It& it : items) {
+      for (int k = 0; k < 4; ++k) {
+        drop(it.seg[k]);
+        drop(it.segp[k]);
+        drop(it.pre[k]);
+      }
+      for (cplx* p : {it.A, it.B, it.Minv, it.b.W, it.b.V, it.b.Wi, it.b.Vi, it.Pb, it.Qb}) drop(p);
+      free_vec(it.b.gam, n);
+    }
+    items.clear();
   };
 
   // ---- 1. forward with checkpoints ----
@@ -564,18 +600,15 @@ void Engine::cell_backward(const std::vector<CellSpec>& cells, const std::vector
     axpby(none, none, Z1, C_ZERO, C_ZERO, 0.0, n);
     axpby(none, none, Z2, C_ZERO, C_ZERO, 0.0, n);
   }
-  for (int j = 0; j < Kmax; ++j) {
-    std::vector<int> act;
+  std::vector<It> items;
+  for (int j0 = 0; j0 < Kmax; j0 += every) {
     for (int c = 0; c < C; ++c)
-      if (j < K[c]) {
-        act.push_back(c);
-        if (j % every == 0) {  // the checkpoint holds the state's pieces
-          const St& s = st[c];
-          ck[c][j] = Ckpt{{s.S[0], s.S[1], s.S[2], s.S[3]}, s.lW, s.lV, s.Pa, s.Qa};
-          for (cplx* p : {s.S[0], s.S[1], s.S[2], s.S[3], s.lW, s.lV, s.Pa, s.Qa}) hold(p);
-        }
+      if (j0 < K[c]) {  // the checkpoint holds the state's pieces
+        const St& s = st[c];
+        ck[c][j0] = Ckpt{{s.S[0], s.S[1], s.S[2], s.S[3]}, s.lW, s.lV, s.Pa, s.Qa};
+        for (cplx* p : {s.S[0], s.S[1], s.S[2], s.S[3], s.lW, s.lV, s.Pa, s.Qa}) hold(p);
       }
-    step(j, act, nullptr);
+    run_block(j0, std::min(Kmax, j0 + every), false, items);
   }
 
   // ---- 2. exit: projection onto the exit basis, reversed ----
@@ -817,16 +850,10 @@ void Engine::cell_backward(const std::vector<CellSpec>& cells, const std::vector
   }
 
   // ---- 3. reverse, block by block from the last checkpoint ----
-  std::vector<int> starts;
-  for (int j0 = 0; j0 < Kmax; j0 += every) starts.push_back(j0);
-  for (int bi = (int)starts.size() - 1; bi >= 0; --bi) {
-    const int j0 = starts[bi], j1 = std::min(Kmax, j0 + every);
-    // restore the checkpoint states (the states take over the checkpoint's
-    // holds) and recompute the block, keeping it
-    std::vector<std::vector<Tape>> tp(j1 - j0);
-    std::vector<std::vector<int>> acts(j1 - j0);
+  for (int j0 = ((Kmax - 1) / every) * every; j0 >= 0; j0 -= every) {
+    const int j1 = std::min(Kmax, j0 + every);
     for (int c = 0; c < C; ++c)
-      if (j0 < K[c]) {
+      if (j0 < K[c]) {  // the states take over the checkpoint's references
         const Ckpt& k = ck[c].at(j0);
         St& s = st[c];
         for (int q = 0; q < 4; ++q) s.S[q] = k.S[q];
@@ -835,34 +862,29 @@ void Engine::cell_backward(const std::vector<CellSpec>& cells, const std::vector
         s.Pa = k.Pa;
         s.Qa = k.Qa;
       }
-    for (int j = j0; j < j1; ++j) {
-      for (int c = 0; c < C; ++c)
-        if (j < K[c]) acts[j - j0].push_back(c);
-      tp[j - j0].resize(acts[j - j0].size());
-      step(j, acts[j - j0], &tp[j - j0]);
-    }
-    // the block's final states: chain S (freed below), samples at its end
+    run_block(j0, j1, true, items);
+    const int NB = (int)items.size();
+    std::map<std::pair<int, int>, int> at;
+    for (int i = 0; i < NB; ++i) at[{items[i].c, items[i].j}] = i;
+    std::vector<std::array<cplx*, 4>> gown(NB);  // own-basis block adjoints of every item
     for (int j = j1 - 1; j >= j0; --j) {
-      const std::vector<int>& act = acts[j - j0];
-      const int B = (int)act.size();
+      std::vector<int> idx;
+      for (int c = 0; c < C; ++c)
+        if (j < K[c]) idx.push_back(at.at({c, j}));
+      const int B = (int)idx.size();
       if (B == 0) continue;
-      std::vector<Tape>& T = tp[j - j0];
       Batch bt{*this, B};
       auto col = [&](auto fn) {
         Vec v(B);
-        for (int q = 0; q < B; ++q) v[q] = fn(T[q]);
+        for (int q = 0; q < B; ++q) v[q] = fn(items[idx[q]]);
         return v;
       };
-      Vec Gs[4];
+      Vec Gs[4], pre[4], sgp[4], sg[4];
       for (int k = 0; k < 4; ++k) {
-        Gs[k].resize(B);
-        for (int q = 0; q < B; ++q) Gs[k][q] = G[k][act[q]];
-      }
-      Vec pre[4], sgp[4], sg[4];
-      for (int k = 0; k < 4; ++k) {
-        pre[k] = col([&](Tape& t) { return t.pre[k]; });
-        sgp[k] = col([&](Tape& t) { return t.segp[k]; });
-        sg[k] = col([&](Tape& t) { return t.seg[k]; });
+        Gs[k] = col([&](It& t) { return G[k][t.c]; });
+        pre[k] = col([&](It& t) { return t.pre[k]; });
+        sgp[k] = col([&](It& t) { return t.segp[k]; });
+        sg[k] = col([&](It& t) { return t.seg[k]; });
       }
       // ---- star product reversed (both operands) ----
       Vec GP[4], gs[4];
@@ -915,43 +937,43 @@ void Engine::cell_backward(const std::vector<CellSpec>& cells, const std::vector
           bt.release(*v, n);
       }
       // ---- left projection reversed (blocks; and its matrices for j = 0) ----
-      Vec gown[4];
-      for (auto& g : gown) g = bt.alloc(n);
+      Vec go[4];
+      for (auto& g : go) g = bt.alloc(n);
       {
-        Vec A = col([](Tape& t) { return t.A; }), Bm = col([](Tape& t) { return t.B; }),
-            Mi = col([](Tape& t) { return t.Minv; });
+        Vec A = col([](It& t) { return t.A; }), Bm = col([](It& t) { return t.B; }),
+            Mi = col([](It& t) { return t.Minv; });
         Vec T1 = bt.alloc(n), T2 = bt.alloc(n), tB = bt.alloc(n), gt2 = bt.alloc(n), gY = bt.alloc(n),
             gM = bt.alloc(n);
         const Vec &gtdd_n = gs[0], &gtuu_n = gs[1], &grud_n = gs[2], &grdu_n = gs[3];
         bt.mm(T1, Bm, sgp[3], C_ONE, 0, 0, &A, C_ONE, n);                      // A + B rdu'
-        bt.mm(gown[1], gtuu_n, T1, C_ONE, 0, 1, nullptr, C_ZERO, n);
+        bt.mm(go[1], gtuu_n, T1, C_ONE, 0, 1, nullptr, C_ZERO, n);
         bt.mm(T2, Bm, sgp[0], C_ONE, 0, 0, nullptr, C_ZERO, n);                // B tdd'
-        bt.mm(gown[1], grud_n, T2, C_ONE, 0, 1, &gown[1], C_ONE, n);           // gtuu
+        bt.mm(go[1], grud_n, T2, C_ONE, 0, 1, &go[1], C_ONE, n);               // gtuu
         bt.mm(tB, sg[1], Bm, C_ONE, 0, 0, nullptr, C_ZERO, n);                 // tuu B
         bt.mm(T1, tB, gtuu_n, C_ONE, 1, 0, &grdu_n, C_ONE, n);                 // grdu' + tB^H gtuu'
         bt.mm(gt2, tB, grud_n, C_ONE, 1, 0, &gtdd_n, C_ONE, n);                // gtdd' + tB^H grud'
-        copy(grud_n, gown[2], n);                                              // grud
-        bt.mm(gown[0], Mi, gt2, C_ONE, 1, 0, nullptr, C_ZERO, n);              // gtdd = M^-H (...)
+        copy(grud_n, go[2], n);                                                // grud
+        bt.mm(go[0], Mi, gt2, C_ONE, 1, 0, nullptr, C_ZERO, n);                // gtdd = M^-H (...)
         bt.mm(gY, Mi, T1, C_ONE, 1, 0, nullptr, C_ZERO, n);                    // gY = M^-H (...)
-        bt.mm(gM, gown[0], sgp[0], C_MONE, 0, 1, nullptr, C_ZERO, n);
+        bt.mm(gM, go[0], sgp[0], C_MONE, 0, 1, nullptr, C_ZERO, n);
         bt.mm(gM, gY, sgp[3], C_MONE, 0, 1, &gM, C_ONE, n);                    // gM = -gtdd tdd'^H - gY rdu'^H
-        bt.mm(gown[3], gY, A, C_ONE, 0, 1, nullptr, C_ZERO, n);
-        bt.mm(gown[3], gM, Bm, C_MONE, 0, 1, &gown[3], C_ONE, n);              // grdu = gY A^H - gM B^H
+        bt.mm(go[3], gY, A, C_ONE, 0, 1, nullptr, C_ZERO, n);
+        bt.mm(go[3], gM, Bm, C_MONE, 0, 1, &go[3], C_ONE, n);                  // grdu = gY A^H - gM B^H
         if (j == 0) {
           // entrance basis: A, B = (Wm^-1 W0 +- Vm^-1 V0) / 2
           std::vector<int> o0;
           for (int q = 0; q < B; ++q)
-            if (own0[act[q]]) o0.push_back(q);
+            if (own0[items[idx[q]].c]) o0.push_back(q);
           if (!o0.empty()) {
             Batch b0{*this, (int)o0.size()};
             Vec gA = b0.alloc(n), gB = b0.alloc(n), S1 = b0.alloc(n), S2 = b0.alloc(n);
             Vec tuu = sub(sg[1], o0), rdu = sub(sg[3], o0), gtuu = sub(gs[1], o0), grud = sub(gs[2], o0),
                 rdun = sub(sgp[3], o0), tddn = sub(sgp[0], o0), gYs = sub(gY, o0), gMs = sub(gM, o0),
-                Wi = sub(col([](Tape& t) { return t.b.Wi; }), o0), Vi = sub(col([](Tape& t) { return t.b.Vi; }), o0);
+                Wi = sub(col([](It& t) { return t.b.Wi; }), o0), Vi = sub(col([](It& t) { return t.b.Vi; }), o0);
             Vec gW(o0.size()), gV(o0.size());
             for (size_t q = 0; q < o0.size(); ++q) {
-              gW[q] = gW0[act[o0[q]]];
-              gV[q] = gV0[act[o0[q]]];
+              gW[q] = gW0[items[idx[o0[q]]].c];
+              gV[q] = gV0[items[idx[o0[q]]].c];
             }
             b0.mm(gA, tuu, gtuu, C_ONE, 1, 0, nullptr, C_ZERO, n);              // tuu^H gtuu'
             b0.mm(S1, gA, rdun, C_ONE, 0, 1, nullptr, C_ZERO, n);               // tuu^H gtuu' rdu'^H
@@ -977,87 +999,112 @@ void Engine::cell_backward(const std::vector<CellSpec>& cells, const std::vector
         }
         for (Vec* v : {&T1, &T2, &tB, &gt2, &gY, &gM}) bt.release(*v, n);
       }
-      // ---- segment formula reversed: node cotangents ----
-      Vec gx[3], gy[3];
-      for (int k = 0; k < 3; ++k) {
-        gx[k] = bt.alloc(n);
-        gy[k] = bt.alloc(n);
-      }
-      {
-        std::vector<NodeAdjDesc> nd(B);
-        for (int q = 0; q < B; ++q) {
-          const int c = act[q];
-          nd[q] = {gown[0][q], gown[1][q], gown[2][q], gown[3][q], T[q].b.gam, {gx[0][q], gx[1][q], gx[2][q]},
-                   {gy[0][q], gy[1][q], gy[2][q]}, cuts[c][j + 1] - cuts[c][j], cells[c].k0()};
-        }
-        Prof pr(*this, "adjoint", 0.0, 160.0 * (double)nn * B);
-        node_adjoint_kernel<<<dim3(grid_for(nn, 256), B), 256, 0, stream_>>>(upload(nd), n);
-        VRC_CUDA_CHECK(cudaGetLastError());
-      }
-      Vec Wm = col([](Tape& t) { return t.b.W; }), Vm = col([](Tape& t) { return t.b.V; }),
-          Wmi = col([](Tape& t) { return t.b.Wi; }), Vmi = col([](Tape& t) { return t.b.Vi; });
-      Vec gP[3], gQ[3], T1 = bt.alloc(n);
-      for (int k = 0; k < 3; ++k) {
-        gP[k] = bt.alloc(n);
-        gQ[k] = bt.alloc(n);
-        bt.mm(T1, Wmi, gx[k], C_ONE, 1, 0, nullptr, C_ZERO, n);
-        bt.mm(gP[k], T1, Vm, C_ONE, 0, 1, nullptr, C_ZERO, n);                 // dL/dP = Wm^-H gx Vm^H
-        bt.mm(T1, Vmi, gy[k], C_ONE, 1, 0, nullptr, C_ZERO, n);
-        bt.mm(gQ[k], T1, Wm, C_ONE, 0, 1, nullptr, C_ZERO, n);                 // dL/dQ = Vm^-H gy Wm^H
-        bt.release(gx[k], n);
-        bt.release(gy[k], n);
-      }
-      bt.release(T1, n);
-      // right node merges with the pending cotangent of the next segment's
-      // left node (or the exit basis at z1); left node becomes pending
-      {
-        std::vector<const cplx*> a, b2;
-        Vec outv;
-        for (int q = 0; q < B; ++q) {
-          const int c = act[q];
-          if (penP[c]) {
-            a.push_back(gP[2][q]);
-            b2.push_back(penP[c]);
-            outv.push_back(gP[2][q]);
-            a.push_back(gQ[2][q]);
-            b2.push_back(penQ[c]);
-            outv.push_back(gQ[2][q]);
-          }
-        }
-        axpby(a, b2, outv, C_ONE, C_ONE, 0.0, n);
-      }
-      std::vector<Node> ns;
       for (int q = 0; q < B; ++q) {
-        const int c = act[q];
-        if (penP[c]) {
-          free_mat(penP[c], n);
-          free_mat(penQ[c], n);
+        const int c = items[idx[q]].c;
+        for (int k = 0; k < 4; ++k) {
+          gown[idx[q]][k] = go[k][q];
+          std::swap(G[k][c], GP[k][q]);  // G <- adjoint of the prefix
         }
-        const double a = cuts[c][j], b = cuts[c][j + 1];
-        ns.push_back({c, 0.5 * (a + b), gP[1][q], gQ[1][q]});
-        ns.push_back({c, b, gP[2][q], gQ[2][q]});
-        penP[c] = gP[0][q];
-        penQ[c] = gQ[0][q];
       }
-      contract(ns);
       for (int k = 0; k < 4; ++k) {
-        for (int q = 0; q < B; ++q) std::swap(G[k][act[q]], GP[k][q]);  // G <- adjoint of the prefix
         bt.release(GP[k], n);
         bt.release(gs[k], n);
-        bt.release(gown[k], n);
       }
     }
-    // release the block: the tape entries and the states after it
-    for (int j = j0; j < j1; ++j)
-      for (Tape& t : tp[j - j0]) {
-        for (int k = 0; k < 4; ++k) {
-          drop(t.pre[k]);
-          drop(t.seg[k]);
-          drop(t.segp[k]);
-        }
-        for (cplx* p : {t.A, t.B, t.Minv, t.b.W, t.b.V, t.b.Wi, t.b.Vi}) drop(p);
-        free_vec(t.b.gam, n);
+    // ---- segment formula reversed for the whole block: node cotangents ----
+    Batch ball{*this, NB};
+    Vec gx[3], gy[3], gP[3], gQ[3];
+    for (int k = 0; k < 3; ++k) {
+      gx[k] = ball.alloc(n);
+      gy[k] = ball.alloc(n);
+    }
+    {
+      std::vector<NodeAdjDesc> nd(NB);
+      for (int i = 0; i < NB; ++i) {
+        const It& it = items[i];
+        nd[i] = {gown[i][0], gown[i][1], gown[i][2], gown[i][3], it.b.gam, {gx[0][i], gx[1][i], gx[2][i]},
+                 {gy[0][i], gy[1][i], gy[2][i]}, cuts[it.c][it.j + 1] - cuts[it.c][it.j], cells[it.c].k0()};
       }
+      Prof pr(*this, "adjoint", 0.0, 160.0 * (double)nn * NB);
+      node_adjoint_kernel<<<dim3(grid_for(nn, 256), NB), 256, 0, stream_>>>(upload(nd), n);
+      VRC_CUDA_CHECK(cudaGetLastError());
+    }
+    for (int i = 0; i < NB; ++i)
+      for (int k = 0; k < 4; ++k) free_mat(gown[i][k], n);
+    {
+      Vec Wm(NB), Vm(NB), Wmi(NB), Vmi(NB), T1 = ball.alloc(n);
+      for (int i = 0; i < NB; ++i) {
+        Wm[i] = items[i].b.W;
+        Vm[i] = items[i].b.V;
+        Wmi[i] = items[i].b.Wi;
+        Vmi[i] = items[i].b.Vi;
+      }
+      for (int k = 0; k < 3; ++k) {
+        gP[k] = ball.alloc(n);
+        gQ[k] = ball.alloc(n);
+        ball.mm(T1, Wmi, gx[k], C_ONE, 1, 0, nullptr, C_ZERO, n);
+        ball.mm(gP[k], T1, Vm, C_ONE, 0, 1, nullptr, C_ZERO, n);               // dL/dP = Wm^-H gx Vm^H
+        ball.mm(T1, Vmi, gy[k], C_ONE, 1, 0, nullptr, C_ZERO, n);
+        ball.mm(gQ[k], T1, Wm, C_ONE, 0, 1, nullptr, C_ZERO, n);               // dL/dQ = Vm^-H gy Wm^H
+        ball.release(gx[k], n);
+        ball.release(gy[k], n);
+      }
+      ball.release(T1, n);
+    }
+    // shared nodes: the right node of segment j meets the left node of j + 1
+    // (inside the block) or the pending cotangent left by the next block (or
+    // by the exit basis); the left node of each cell's first segment here
+    // becomes the pending one
+    {
+      std::vector<const cplx*> a, b2;
+      Vec outv;
+      for (int i = 0; i < NB; ++i) {
+        const It& it = items[i];
+        const cplx *addP = nullptr, *addQ = nullptr;
+        auto nx = at.find({it.c, it.j + 1});
+        if (nx != at.end()) {
+          addP = gP[0][nx->second];
+          addQ = gQ[0][nx->second];
+        } else if (penP[it.c]) {
+          addP = penP[it.c];
+          addQ = penQ[it.c];
+        }
+        if (addP) {
+          a.push_back(gP[2][i]);
+          b2.push_back(addP);
+          outv.push_back(gP[2][i]);
+          a.push_back(gQ[2][i]);
+          b2.push_back(addQ);
+          outv.push_back(gQ[2][i]);
+        }
+      }
+      axpby(a, b2, outv, C_ONE, C_ONE, 0.0, n);
+    }
+    std::vector<Node> ns;
+    for (int i = 0; i < NB; ++i) {
+      const It& it = items[i];
+      const double za = cuts[it.c][it.j], zb = cuts[it.c][it.j + 1];
+      ns.push_back({it.c, 0.5 * (za + zb), gP[1][i], gQ[1][i]});
+      ns.push_back({it.c, zb, gP[2][i], gQ[2][i]});
+    }
+    for (int c = 0; c < C; ++c)
+      if (j0 < K[c] && penP[c]) {
+        free_mat(penP[c], n);
+        free_mat(penQ[c], n);
+        penP[c] = penQ[c] = nullptr;
+      }
+    for (int i = 0; i < NB; ++i) {
+      const It& it = items[i];
+      if (it.j == j0) {
+        penP[it.c] = gP[0][i];
+        penQ[it.c] = gQ[0][i];
+      } else {
+        free_mat(gP[0][i], n);
+        free_mat(gQ[0][i], n);
+      }
+    }
+    contract(ns);
+    release_items(items);
     for (int c = 0; c < C; ++c)
       if (j0 < K[c]) {
         St& s = st[c];
@@ -1113,7 +1160,6 @@ void Engine::cell_backward(const std::vector<CellSpec>& cells, const std::vector
 
   // ---- release ----
   if (dLdx) free_bytes(dLdx, dLdx_cap * sizeof(double));
-  free_bytes(derr, (size_t)C * sizeof(double));
   for (int c = 0; c < C; ++c) {
     for (cplx* p : {P0[c], Q0[c], P1[c], Q1[c], last[c].Wi, last[c].Vi}) drop(p);
     drop_bas(e0[c]);

@@ -18,7 +18,7 @@ def cell_seeds(workload: str, batch: int, rank: int, step_seed: int = 0) -> List
     rank so that replicas never solve the same cell."""
     if batch > RANK_STRIDE:
         raise ValueError("batch per rank exceeds the seed stride")
-    base = 1000 * {"c1": 1, "c2": 2, "c3": 3, "c4": 4}[workload] + RANK_STRIDE * rank + step_seed
+    base = 1000 * {"c1": 1, "c2": 2, "c3": 3, "c4": 4, "c5": 5}[workload] + RANK_STRIDE * rank + step_seed
     return [base + i for i in range(batch)]
 
 
@@ -33,6 +33,8 @@ def make_cells(workload: str, batch: int, rank: int, npix: int, step_seed: int =
         return [st.pillar_config2(seed=s, npix=npix) for s in seeds]
     if workload == "c4":  # freeform metagrating stacks (npix is the 256 raster of c2/c3; c4 keeps 64x64)
         return [st.metagrating_c4(seed=s, norders=orders) for s in seeds]
+    if workload == "c5":  # PML mode converters (orders: harmonics per axis, 21 = config 5)
+        return [st.converter_c5(s, norders=orders) for s in seeds]
     return [st.pillar_config3(seed=s, npix=npix) for s in seeds]
 
 

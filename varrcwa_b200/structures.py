@@ -136,10 +136,11 @@ def pillar_config3(seed, npix=256):
 
 def waveguide_pml(seed, norders=21, ncontrol=64, length=20.0, cell=(4.0, 2.0),
                   pml=0.5, eps_core=EPS_SI_BENCH, eps_clad=EPS_SIO2_BENCH, lam=1.55,
-                  core_h=0.22):
+                  core_h=0.22, spline=False):
     """Waveguide mode converter with PML on both lateral boundaries: the core
-    width follows a piecewise-linear interpolation of seeded control points
-    (cubic-spline tables are tabulated to piecewise-linear knots)."""
+    width follows seeded control points, interpolated piecewise-linearly or
+    (spline=True, config 5) by the natural cubic spline; the two core edges
+    are the moving coordinates, cx -+ w(z) / 2."""
     rng = np.random.default_rng(seed)
     widths = rng.uniform(0.3, 1.2, size=ncontrol)
     zs = np.linspace(0.0, length, ncontrol)
@@ -152,7 +153,14 @@ def waveguide_pml(seed, norders=21, ncontrol=64, length=20.0, cell=(4.0, 2.0),
     eps[2, 2] = s
     return dict(kind="grid", lam=lam, nx=norders, ny=norders, pml=True, x=x, y=y, eps=eps,
                 xrules=[(2, zs, cx - 0.5 * widths), (3, zs, cx + 0.5 * widths)],
-                z0=0.0, z1=length, end0=None, end1=None, widths=widths)
+                z0=0.0, z1=length, end0=None, end1=None, widths=widths, spline=bool(spline))
+
+
+def converter_c5(seed, norders=21, ncontrol=64, length=20.0):
+    """Config 5: 4 x 2 um cell, PML 0.5 um, Si core in SiO2, width over 20 um
+    through 64 seeded control points U[0.3, 1.2] um, natural cubic spline,
+    21 x 21 orders (n = 882)."""
+    return waveguide_pml(seed, norders=norders, ncontrol=ncontrol, length=length, spline=True)
 
 
 def smooth_pixels(seed, npx, npy, sigma=3.0, beta=8.0, lo=2.085, hi=12.11):
