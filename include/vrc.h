@@ -249,6 +249,42 @@ int vrc_rcwa(vrc_context* ctx, int ncells, const vrc_cell* cells, int N, vrc_res
  * (src/core/DifferentialIntegrator.cpp:21-134). */
 int vrc_differential(vrc_context* ctx, int ncells, const vrc_cell* cells, int N, vrc_result* results);
 
+/* ---- stacks of sections ---------------------------------------------------------
+ * A stack of nsections cells, each on its own z-range, solved in order along
+ * z: RCWASolver::solve(lambda, layerStack, thickness)
+ * (src/rcwa/RCWASolver.cpp:104-113) for layers that may vary with z, so
+ * adaptive varRCWA sections and z-uniform layers mix.  Every section is
+ * integrated (method 0: adaptive varRCWA with pe, max_depth; 1: RCWA, 2:
+ * the differential method, with nslices), all sections as one batch; then
+ * the sections are joined in order, each section's entrance re-expressed in
+ * the previous section's exit basis (matching the transverse fields W c,
+ * V c of the two sides, as RCWASolver's interface matrices do, :460-580)
+ * and star-multiplied (:343-458).  The first section's has_end0 and the
+ * last's has_end1 set the outer media (the others' end flags are ignored);
+ * all sections need the same nx, ny and periods.  result: the stack's
+ * blocks, the entrance basis (W0, V0, gam0) and the exit basis (W1, V1,
+ * gam1), with N, n_eig ... summed over the sections; vrc_get_tree(ctx, s)
+ * gives section s's segmentation.  The stack stays on the device for
+ * vrc_chain_order_powers and vrc_chain_fields until the next vrc_chain. */
+int vrc_chain(vrc_context* ctx, int nsections, const vrc_cell* sections, int method, double pe, int max_depth,
+              int nslices, vrc_result* result);
+/* Per-order powers of the last stack (vrc_order_powers' side, flux_norm and
+ * layout for one cell: R, T of 2 * nx*ny doubles); needs half-space ends and
+ * periodic boundaries (RCWASolver::scatterPlaneWave, :1636-1733). */
+int vrc_chain_order_powers(vrc_context* ctx, int side, int flux_norm, double* R, double* T);
+/* Mode amplitudes at every interface of the last stack for incident
+ * amplitudes c (n, in the entrance basis, going up): interface j = 0 ..
+ * nsections is the entrance of section j (j = nsections: the exit); amps
+ * holds per interface the up- then the down-going amplitudes in the basis of
+ * the region below it (j = 0: incident and reflected; j = nsections:
+ * transmitted and zero) -- (nsections + 1) * 2 * n -- the role of
+ * RCWASolver::evaluateIntermediateField (:1373-1480).  With ngx, ngy > 0,
+ * fields ((nsections + 1) * 2 * ngy * ngx: Ex then Ey, rows of constant y)
+ * samples the transverse E field over the period there (fields may be NULL
+ * otherwise).  Fields inside a section: split it into two sections there. */
+int vrc_chain_fields(vrc_context* ctx, const vrc_complex* c, int ngx, int ngy, vrc_complex* amps,
+                     vrc_complex* fields);
+
 /* ---- A14: per-order power -----------------------------------------------------
  * Integrate (method 0: adaptive varRCWA with pe/max_depth, 1: RCWA with
  * N = nslices, 2: differential with N) and return per-order reflected /

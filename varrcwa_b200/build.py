@@ -28,7 +28,7 @@ LIB = PKG / "libvrc.so"
 STAMP = PKG / "libvrc.so.sha"
 
 SOURCES = ["gemm.cu", "inverse.cu", "eig.cu", "hessenberg.cu", "qr.cu", "assembly.cu", "segment.cu", "engine.cu",
-           "drivers.cu", "capi.cu", "noalloc.cu", "adjoint.cu", "stack.cu", "gds.cu", "geom_adjoint.cu"]
+           "drivers.cu", "capi.cu", "noalloc.cu", "adjoint.cu", "stack.cu", "gds.cu", "geom_adjoint.cu", "chain.cu"]
 HEADERS = ["common.cuh", "kernels.h", "engine.h", "householder.cuh", "batch.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",

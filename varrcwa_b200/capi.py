@@ -25,6 +25,7 @@ EXPORTS = [
     "vrc_differential", "vrc_order_powers", "vrc_zgemm", "vrc_zinv", "vrc_set_profiling",
     "vrc_get_kernel_stats", "vrc_eig_noalloc", "vrc_stack_forward", "vrc_stack_backward", "vrc_gds_read",
     "vrc_planar_section", "vrc_stack_fields", "vrc_redheffer_forward", "vrc_redheffer_backward",
+    "vrc_chain", "vrc_chain_order_powers", "vrc_chain_fields",
 ]
 
 
@@ -141,6 +142,10 @@ def lib():
     L.vrc_redheffer_forward.argtypes = [vp, C.c_int, C.POINTER(VrcCell), C.c_double, C.c_int,
                                         C.POINTER(VrcResult)]
     L.vrc_redheffer_backward.argtypes = [vp, CP, CP, C.c_int, DP]
+    L.vrc_chain.argtypes = [vp, C.c_int, C.POINTER(VrcCell), C.c_int, C.c_double, C.c_int, C.c_int,
+                            C.POINTER(VrcResult)]
+    L.vrc_chain_order_powers.argtypes = [vp, C.c_int, C.c_int, DP, DP]
+    L.vrc_chain_fields.argtypes = [vp, CP, C.c_int, C.c_int, CP, CP]
     _lib = L
     return L
 
@@ -542,6 +547,37 @@ class Context:
                         "status": int(st[i])})
             off += 2 * m
         return out
+
+    # ---- stacks of sections ----
+    def chain(self, descs: List[dict], method: str = "redheffer", pe: float = 1e-2, max_depth: int = 40,
+              nslices: int = 10):
+        """Sections (each a structure on its own z-range) solved and joined in
+        order; returns the stack's result dict (blocks, entrance and exit bases)."""
+        packs = [_CellPack(d) for d in descs]
+        cells = (VrcCell * len(descs))(*[p.cell for p in packs])
+        res, bufs = self._results(descs[:1], True)
+        meth = {"redheffer": 0, "rcwa": 1, "differential": 2}[method]
+        self._check(self.L.vrc_chain(self.h, len(descs), cells, meth, float(pe), int(max_depth), int(nslices), res))
+        self._chain = (len(descs), 2 * descs[0]["nx"] * descs[0]["ny"], descs[0]["nx"] * descs[0]["ny"])
+        return self._unpack(res, bufs)[0]
+
+    def chain_order_powers(self, side: int = 1, flux_norm: bool = True):
+        _, _, m = self._chain
+        R = np.zeros(2 * m)
+        T = np.zeros(2 * m)
+        self._check(self.L.vrc_chain_order_powers(self.h, int(side), 1 if flux_norm else 0, _dptr(R), _dptr(T)))
+        return {"R": R.reshape(2, m), "T": T.reshape(2, m)}
+
+    def chain_fields(self, c, ngx: int = 0, ngy: int = 0):
+        """Interface amplitudes (S+1, 2, n) for incident entrance amplitudes c,
+        and Ex / Ey images (S+1, 2, ngy, ngx) when ngx, ngy > 0."""
+        S, n, _ = self._chain
+        c = np.ascontiguousarray(c, dtype=np.complex128)
+        amps = np.zeros((S + 1, 2, n), dtype=np.complex128)
+        img = np.zeros((S + 1, 2, ngy, ngx), dtype=np.complex128) if ngx > 0 else None
+        self._check(self.L.vrc_chain_fields(self.h, _cptr(c), int(ngx), int(ngy), amps.ctypes.data_as(CP),
+                                            img.ctypes.data_as(CP) if img is not None else None))
+        return amps, img
 
     # ---- layer stacks: forward and adjoint ----
     def stack_forward(self, stacks: List[dict], px: float = 1.0, py: float = 0.0):

@@ -670,6 +670,63 @@ int vrc_redheffer_backward(vrc_context* ctx, const vrc_complex* gS, const vrc_co
   });
 }
 
+int vrc_chain(vrc_context* ctx, int nsections, const vrc_cell* sections, int method, double pe, int max_depth,
+              int nslices, vrc_result* result) {
+  return guarded(ctx, [&] {
+    if (nsections < 1 || !result) throw vrc::StatusError(VRC_EINVAL, "invalid arguments");
+    if (method == 0 && (!(pe > 0.0) || max_depth < 0))
+      throw vrc::StatusError(VRC_EINVAL, "pe must be > 0 and max_depth >= 0");
+    if (method != 0 && nslices < 1) throw vrc::StatusError(VRC_EINVAL, "nslices must be >= 1");
+    auto specs = to_specs(nsections, sections);
+    vrc::Engine& E = *ctx->eng;
+    vrc::CellResult r;
+    Timed tm(ctx);
+    E.chain(specs, method, pe, max_depth, nslices, r, ctx->trees);
+    tm.done();
+    const size_t nn = (size_t)r.n * r.n * 16, nv = (size_t)r.n * 16;
+    vrc_result& o = *result;
+    d2h(o.Tdd, r.Tdd, nn, E.stream());
+    d2h(o.Tuu, r.Tuu, nn, E.stream());
+    d2h(o.Rud, r.Rud, nn, E.stream());
+    d2h(o.Rdu, r.Rdu, nn, E.stream());
+    d2h(o.W0, r.W0, nn, E.stream());
+    d2h(o.V0, r.V0, nn, E.stream());
+    d2h(o.gam0, r.gam0, nv, E.stream());
+    d2h(o.W1, r.W1, nn, E.stream());
+    d2h(o.V1, r.V1, nn, E.stream());
+    d2h(o.gam1, r.gam1, nv, E.stream());
+    E.sync();
+    o.status = r.status;
+    o.n = r.n;
+    o.N = r.N;
+    o.n_eig = r.n_eig;
+    o.n_samples = r.n_samples;
+    o.n_nodes = r.n_nodes;
+  });
+}
+
+int vrc_chain_order_powers(vrc_context* ctx, int side, int flux_norm, double* R, double* T) {
+  return guarded(ctx, [&] {
+    if (!R || !T || (side != 0 && side != 1)) throw vrc::StatusError(VRC_EINVAL, "invalid arguments");
+    std::vector<double> r, t;
+    ctx->eng->chain_order_powers(side, flux_norm, r, t);
+    std::memcpy(R, r.data(), r.size() * sizeof(double));
+    std::memcpy(T, t.data(), t.size() * sizeof(double));
+  });
+}
+
+int vrc_chain_fields(vrc_context* ctx, const vrc_complex* c, int ngx, int ngy, vrc_complex* amps,
+                     vrc_complex* fields) {
+  return guarded(ctx, [&] {
+    if (!c || !amps || ngx < 0 || ngy < 0 || ((ngx > 0) != (ngy > 0)) || (ngx > 0 && !fields))
+      throw vrc::StatusError(VRC_EINVAL, "invalid arguments");
+    Timed tm(ctx);
+    ctx->eng->chain_fields(reinterpret_cast<const cplx*>(c), ngx, ngy, reinterpret_cast<cplx*>(amps),
+                           ngx > 0 ? reinterpret_cast<cplx*>(fields) : nullptr);
+    tm.done();
+  });
+}
+
 int vrc_get_tree(vrc_context* ctx, int cell, int max_nodes, double* a, double* b, double* err, int* accepted) {
   if (!ctx || cell < 0 || cell >= (int)ctx->trees.size()) return -VRC_EINVAL;
   const auto& t = ctx->trees[cell];

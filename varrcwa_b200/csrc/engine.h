@@ -2,6 +2,7 @@
 // the varRCWA hot path, driven from C++ (no host-side math on the path).
 #pragma once
 
+#include <array>
 #include <functional>
 #include <map>
 #include <memory>
@@ -415,8 +416,32 @@ class Engine {
   };
   const StackTape& stack_tape() const { return tape_; }
 
+  // ---- stacks of sections (each a cell on its own z-range) ----
+  struct ChainTape {
+    int n = 0, m = 0;
+    std::vector<CellResult> secs;               // every section's result
+    std::vector<std::array<cplx*, 4>> proj;    // blocks, entrance in the previous exit basis
+    std::vector<std::array<cplx*, 4>> prefix;  // chain of sections 0..s
+    std::vector<cplx*> V0inv;                  // sections 1..
+    double *alpha = nullptr, *beta = nullptr;  // harmonics (field images)
+    double Lx = 1.0, Ly = 1.0;
+    CellSpec spec;      // outer media of the stack (order powers)
+    CellResult result;  // points into secs / prefix
+  };
+  // Solves the sections (method 0 adaptive varRCWA, 1 RCWA, 2 differential)
+  // and joins them; out points into the kept stack (valid until the next
+  // chain); trees: every section's segmentation.
+  void chain(const std::vector<CellSpec>& sections, int method, double pe, int max_depth, int nslices,
+             CellResult& out, std::vector<std::vector<NodeRecord>>& trees);
+  void chain_order_powers(int side, int flux_norm, std::vector<double>& R, std::vector<double>& T);
+  // amplitudes (a+, a-) at every interface for incident entrance amplitudes
+  // c (host, n); amps: (S+1) x 2 x n, img: (S+1) x 2 x ngy x ngx or null
+  void chain_fields(const cplx* c, int ngx, int ngy, cplx* amps, cplx* img);
+  void release_chain();
+
  private:
   StackTape tape_;
+  ChainTape chain_;
 };
 
 template <class T>
