@@ -231,11 +231,12 @@ __global__ void gather_fe_kernel(const cplx* const* __restrict__ G11s, const cpl
 // ---------------------------------------------------------------------------
 __global__ void assemble_periodic_kernel(const cplx* const* __restrict__ finvs,
                                          const cplx* const* __restrict__ fe11s,
-                                         const cplx* const* __restrict__ fe22s,
-                                         const double* __restrict__ alpha, const double* __restrict__ beta,
+                                         const cplx* const* __restrict__ fe22s, const double* __restrict__ ab,
                                          const double* __restrict__ k0sq, cplx* const* __restrict__ Ps,
                                          cplx* const* __restrict__ Qs, int m) {
   const int s = blockIdx.y;
+  const double* alpha = ab + (size_t)s * 2 * m;  // per sample: alpha then beta
+  const double* beta = alpha + m;
   const cplx* f = finvs[s];
   const cplx* f11 = fe11s[s];
   const cplx* f22 = fe22s[s];
@@ -270,12 +271,13 @@ __global__ void assemble_periodic_kernel(const cplx* const* __restrict__ finvs,
 __global__ void assemble_dense_kernel(const cplx* const* __restrict__ KxF2h, const cplx* const* __restrict__ KxF1h,
                                       const cplx* const* __restrict__ KyF2h, const cplx* const* __restrict__ KyF1h,
                                       const cplx* const* __restrict__ fe11s, const cplx* const* __restrict__ fe22s,
-                                      const cplx* __restrict__ KxKy, const cplx* __restrict__ KxKx,
-                                      const cplx* __restrict__ KyKy, const cplx* __restrict__ KyKx,
+                                      const cplx* const* __restrict__ KxKys, const cplx* const* __restrict__ KxKxs,
+                                      const cplx* const* __restrict__ KyKys, const cplx* const* __restrict__ KyKxs,
                                       const double* __restrict__ k0sq, cplx* const* __restrict__ Ps,
                                       cplx* const* __restrict__ Qs, int m) {
   const int s = blockIdx.y;
   const double k02 = k0sq[s];
+  const cplx *KxKy = KxKys[s], *KxKx = KxKxs[s], *KyKy = KyKys[s], *KyKx = KyKxs[s];
   const int n = 2 * m;
   cplx* P = Ps[s];
   cplx* Q = Qs[s];
@@ -354,18 +356,19 @@ void gather_fe(const cplx* const* d_G11, const cplx* const* d_G22, const cplx* c
 }
 
 void assemble_periodic(const cplx* const* d_finv, const cplx* const* d_fe11, const cplx* const* d_fe22,
-                       const double* d_alpha, const double* d_beta, const double* d_k0sq, cplx* const* d_P,
-                       cplx* const* d_Q, int m, int batch, cudaStream_t st) {
+                       const double* d_ab, const double* d_k0sq, cplx* const* d_P, cplx* const* d_Q, int m, int batch,
+                       cudaStream_t st) {
   if (batch <= 0) return;
-  assemble_periodic_kernel<<<grid_for(m * m, batch), 256, 0, st>>>(d_finv, d_fe11, d_fe22, d_alpha, d_beta,
-                                                                   d_k0sq, d_P, d_Q, m);
+  assemble_periodic_kernel<<<grid_for(m * m, batch), 256, 0, st>>>(d_finv, d_fe11, d_fe22, d_ab, d_k0sq, d_P, d_Q,
+                                                                   m);
   VRC_CUDA_CHECK(cudaGetLastError());
 }
 
 void assemble_dense(const cplx* const* KxF2h, const cplx* const* KxF1h, const cplx* const* KyF2h,
-                    const cplx* const* KyF1h, const cplx* const* fe11, const cplx* const* fe22, const cplx* KxKy,
-                    const cplx* KxKx, const cplx* KyKy, const cplx* KyKx, const double* d_k0sq, cplx* const* d_P,
-                    cplx* const* d_Q, int m, int batch, cudaStream_t st) {
+                    const cplx* const* KyF1h, const cplx* const* fe11, const cplx* const* fe22,
+                    const cplx* const* KxKy, const cplx* const* KxKx, const cplx* const* KyKy,
+                    const cplx* const* KyKx, const double* d_k0sq, cplx* const* d_P, cplx* const* d_Q, int m,
+                    int batch, cudaStream_t st) {
   if (batch <= 0) return;
   assemble_dense_kernel<<<grid_for(m * m, batch), 256, 0, st>>>(KxF2h, KxF1h, KyF2h, KyF1h, fe11, fe22, KxKy, KxKx,
                                                                 KyKy, KyKx, d_k0sq, d_P, d_Q, m);

@@ -950,21 +950,10 @@ void Engine::assemble_grid(std::vector<SampleReq>& reqs, std::vector<int>* statu
         }
         double* dab = upload(ab);
         double* dk = upload(k0sq);
-        // one launch per distinct alpha/beta would be simplest; instead the
-        // kernel indexes per sample through a strided layout
-        for (size_t b = 0; b < B; ++b) {
-          // batch of consecutive samples sharing the same cell constants
-          size_t e = b + 1;
-          while (e < B && reqs[idx[c0 + e]].cd == reqs[idx[c0 + b]].cd) ++e;
-          std::vector<const cplx*> fi(fe33.begin() + b, fe33.begin() + e);
-          std::vector<const cplx*> f1(fe11.begin() + b, fe11.begin() + e);
-          std::vector<const cplx*> f2v(fe22.begin() + b, fe22.begin() + e);
-          std::vector<cplx*> pv(Pp.begin() + b, Pp.begin() + e), qv(Qp.begin() + b, Qp.begin() + e);
-          Prof pr(*this, "assembly", 0.0, 16.0 * (e - b) * (3.0 * m * m + 8.0 * m * m));
-          assemble_periodic(upload(fi), upload(f1), upload(f2v), dab + b * 2 * m, dab + b * 2 * m + m, dk + b,
-                            upload(pv), upload(qv), m, (int)(e - b), stream_);
-          b = e - 1;
-        }
+        std::vector<const cplx*> fi(fe33.begin(), fe33.end()), f1(fe11.begin(), fe11.end()),
+            f2v(fe22.begin(), fe22.end());
+        Prof pr(*this, "assembly", 0.0, 16.0 * B * (3.0 * m * m + 8.0 * m * m));
+        assemble_periodic(upload(fi), upload(f1), upload(f2v), dab, dk, upload(Pp), upload(Qp), m, (int)B, stream_);
       } else {
         auto F1h = ptrs(o_pml), F2h = ptrs(o_pml + (size_t)m * m), KxF2h = ptrs(o_pml + 2 * (size_t)m * m),
              KxF1h = ptrs(o_pml + 3 * (size_t)m * m), KyF2h = ptrs(o_pml + 4 * (size_t)m * m),
@@ -985,18 +974,19 @@ void Engine::assemble_grid(std::vector<SampleReq>& reqs, std::vector<int>* statu
         }
         gemm(g2, m, mk(1, 0), mk(0, 0), 0.0);
         double* dk = upload(k0sq);
+        std::vector<const cplx*> kxky(B), kxkx(B), kyky(B), kykx(B);
         for (size_t b = 0; b < B; ++b) {
-          size_t e = b + 1;
-          while (e < B && reqs[idx[c0 + e]].cd == reqs[idx[c0 + b]].cd) ++e;
           const CellDev* cd = reqs[idx[c0 + b]].cd;
-          auto sl = [&](const std::vector<cplx*>& v) { return std::vector<const cplx*>(v.begin() + b, v.begin() + e); };
-          std::vector<cplx*> pv(Pp.begin() + b, Pp.begin() + e), qv(Qp.begin() + b, Qp.begin() + e);
-          Prof pr(*this, "assembly", 0.0, 16.0 * (e - b) * (6.0 * m * m + 8.0 * m * m));
-          assemble_dense(upload(sl(KxF2h)), upload(sl(KxF1h)), upload(sl(KyF2h)), upload(sl(KyF1h)), upload(sl(fe11)),
-                         upload(sl(fe22)), cd->KxKy, cd->KxKx, cd->KyKy, cd->KyKx, dk + b, upload(pv), upload(qv), m,
-                         (int)(e - b), stream_);
-          b = e - 1;
+          kxky[b] = cd->KxKy;
+          kxkx[b] = cd->KxKx;
+          kyky[b] = cd->KyKy;
+          kykx[b] = cd->KyKx;
         }
+        auto cv = [](const std::vector<cplx*>& v) { return std::vector<const cplx*>(v.begin(), v.end()); };
+        Prof pr(*this, "assembly", 0.0, 16.0 * B * (6.0 * m * m + 8.0 * m * m));
+        assemble_dense(upload(cv(KxF2h)), upload(cv(KxF1h)), upload(cv(KyF2h)), upload(cv(KyF1h)), upload(cv(fe11)),
+                       upload(cv(fe22)), upload(kxky), upload(kxkx), upload(kyky), upload(kykx), dk, upload(Pp),
+                       upload(Qp), m, (int)B, stream_);
       }
       if (status) {
         std::vector<int> h(B);

@@ -66,13 +66,16 @@ void toeplitz_inverses(const cplx* const* d_F, cplx* const* d_out, int t, int nm
                        cudaStream_t st);
 void gather_fe(const cplx* const* d_G11, const cplx* const* d_G22, const cplx* const* d_F2, cplx* const* d_fe11,
                cplx* const* d_fe22, cplx* const* d_fe33, int nx, int ny, int batch, cudaStream_t st);
+// d_ab: per sample alpha (m) then beta (m), 2 m doubles per sample
 void assemble_periodic(const cplx* const* d_finv, const cplx* const* d_fe11, const cplx* const* d_fe22,
-                       const double* d_alpha, const double* d_beta, const double* d_k0sq, cplx* const* d_P,
-                       cplx* const* d_Q, int m, int batch, cudaStream_t st);
+                       const double* d_ab, const double* d_k0sq, cplx* const* d_P, cplx* const* d_Q, int m, int batch,
+                       cudaStream_t st);
+// KxKy ... KyKx: per sample (each sample's cell constants)
 void assemble_dense(const cplx* const* KxF2h, const cplx* const* KxF1h, const cplx* const* KyF2h,
-                    const cplx* const* KyF1h, const cplx* const* fe11, const cplx* const* fe22, const cplx* KxKy,
-                    const cplx* KxKx, const cplx* KyKy, const cplx* KyKx, const double* d_k0sq, cplx* const* d_P,
-                    cplx* const* d_Q, int m, int batch, cudaStream_t st);
+                    const cplx* const* KyF1h, const cplx* const* fe11, const cplx* const* fe22,
+                    const cplx* const* KxKy, const cplx* const* KxKx, const cplx* const* KyKy,
+                    const cplx* const* KyKx, const double* d_k0sq, cplx* const* d_P, cplx* const* d_Q, int m,
+                    int batch, cudaStream_t st);
 
 // ---- segment / elementwise ------------------------------------------------------
 struct SegDesc {
