@@ -5,7 +5,9 @@ not acceptable).  Its scratch is a fixed area inside the library.
 
 Checked through the C-ABI, twice in a row (so that the second call runs on
 the scratch left by the first):
-* against vrc_eig (the allocating entry point) on the same matrices;
+* against vrc_eig (the allocating entry point) on the same matrices,
+  eigenvalues matched (their order may differ) at the eigensolver tests'
+  tolerance and the normalised eigenvectors to 1e-10;
 * directly: the residual ||A W - W diag(lam)|| and the eigenvalues against
   numpy's (LAPACK zgeev), unit-norm columns;
 * that a warmed-up call leaves the device's free memory and torch's
@@ -19,7 +21,6 @@ import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
-TOL = 1e-12
 
 
 def _dev(a, torch):
@@ -64,8 +65,18 @@ def test_eig_noalloc_matches_eig_twice(ctx, n):
         W = dW.cpu().numpy().T
         lam = dlam.cpu().numpy()
         assert np.all(np.isfinite(W)) and np.all(np.isfinite(lam))
-        assert np.abs(lam - lam_ref).max() <= TOL * np.abs(lam_ref).max(), call
-        assert np.abs(W - W_ref).max() <= TOL, call
+        # the allocating entry point may order the eigenvalues differently
+        # (its Hessenberg reduction is blocked for larger n): match them, then
+        # the unit, largest-component-real eigenvector columns
+        scale = np.abs(A).max()
+        order = []
+        free = list(range(n))
+        for x in lam:
+            k = min(free, key=lambda q: abs(lam_ref[q] - x))
+            order.append(k)
+            free.remove(k)
+        assert np.abs(lam - lam_ref[order]).max() <= 1e-12 * scale * n, call
+        assert np.abs(W - W_ref[:, order]).max() <= 1e-10, call
         # directly: A W = W diag(lam), unit columns, eigenvalues of LAPACK's zgeev
         scale = np.linalg.norm(A, 2)
         res = np.linalg.norm(A @ W - W * lam[None, :], 2)

@@ -1008,6 +1008,14 @@ void Engine::assemble_grid(std::vector<SampleReq>& reqs, std::vector<int>* statu
 // ---------------------------------------------------------------------------
 // Eigen-decomposition of PQ (A7)
 // ---------------------------------------------------------------------------
+// Blocked Hessenberg reduction (panels + DMMA GEMM updates) from this order
+// up; the single-CTA / cluster kernels below it.  VRC_HESS_BLOCKED=0 / 1
+// turns it off / on for every order.
+static bool use_blocked_hessenberg(int n) {
+  if (const char* e = std::getenv("VRC_HESS_BLOCKED")) return std::atoi(e) != 0 && n >= 3;
+  return n >= 128;
+}
+
 void Engine::eig(std::vector<EigReq>& reqs, int n, std::vector<int>* status) {
   if (reqs.empty()) return;
   const size_t logc = schur_log_bytes(n) / 16;  // rotation log, complex units
@@ -1051,7 +1059,23 @@ void Engine::eig(std::vector<EigReq>& reqs, int n, std::vector<int>* status) {
     const double nn3 = (double)n * n * n, mbytes = 16.0 * n * (double)n;
     {
       Prof pr(*this, "hessenberg", (56.0 / 3.0) * nn3 * B, 3.0 * mbytes * B);
-      hessenberg_batched(upload(H), upload(Z), (int)B, n, stream_);
+      if (use_blocked_hessenberg(n)) {
+        // panels with DMMA GEMM updates; the panel scratch lives in each
+        // matrix's Y block (free until the back substitution) when it fits
+        const size_t need = hessenberg_blocked_scratch(n);
+        const bool in_y = need <= (size_t)n * n * 16;
+        for (size_t b0 = 0; b0 < B; b0 += 65535) {
+          const size_t nb = std::min<size_t>(65535, B - b0);
+          void* scr = in_y ? (void*)Y[b0] : bytes(nb * need);
+          void* dd = bytes(hessenberg_blocked_descs((int)nb));
+          std::vector<cplx*> hb(H.begin() + b0, H.begin() + b0 + nb), zb(Z.begin() + b0, Z.begin() + b0 + nb);
+          hessenberg_blocked_batched(upload(hb), upload(zb), (int)nb, n, scr, in_y ? per * 16 : need, dd, stream_);
+          free_bytes(dd, hessenberg_blocked_descs((int)nb));
+          if (!in_y) free_bytes(scr, nb * need);
+        }
+      } else {
+        hessenberg_batched(upload(H), upload(Z), (int)B, n, stream_);
+      }
     }
     int* dstat = (int*)bytes(B * sizeof(int));
     VRC_CUDA_CHECK(cudaMemsetAsync(dstat, 0, B * sizeof(int), stream_));

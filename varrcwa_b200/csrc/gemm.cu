@@ -5,8 +5,10 @@
 // for column-major n x n operands (every contraction of the hot path is
 // square: projections, star products, perturbation terms, P*Q), or with an
 // inner dimension kdim != n (A is n x kdim, B is kdim x n) for the rank-kdim
-// updates of the blocked inversion.  Either operand may be taken as its
-// conjugate transpose (square operands only; used by the adjoint).  One CTA
+// updates of the blocked inversion, or of general shape M x N x K with
+// leading dimensions (zgemm_rect_batched: the panel updates of the blocked
+// Hessenberg reduction).  Either operand may be taken as its conjugate
+// transpose (used by the adjoint and the Hessenberg reflectors).  One CTA
 // computes a 64 x 64 complex tile (eight warps of 32 x 16), or a 32 x 32
 // tile (four warps of 16 x 16) for small orders, where 64-wide tiles would
 // mostly compute padding (n = 82: 41% of a 128 x 128 cover is useful, 73% of
@@ -61,12 +63,19 @@ __device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, doubl
       : "d"(a0), "d"(a1), "d"(b0));
 }
 
+// Shape of a batched product: C (M x N, ldc) = op(A) (M x K) op(B) (K x N);
+// A stored M x K (lda) or, transposed, K x M; B stored K x N (ldb) or N x K.
+struct GemmShape {
+  int M, N, K, lda, ldb, ldc;
+};
+
 // OPA / OPB: 0 = the operand as stored, 1 = its conjugate transpose.  A
 // transposed operand is staged with consecutive threads along its stored
 // columns (coalesced) and conjugated when fragments are read.
+
 template <class TL, int OPA, int OPB>
 __global__ void __launch_bounds__(TL::THREADS, 512 / TL::THREADS)
-    zgemm_kernel(const GemmDesc* __restrict__ descs, int n, int kdim, cplx alpha, cplx beta, double delta) {
+    zgemm_kernel(const GemmDesc* __restrict__ descs, GemmShape sh, cplx alpha, cplx beta, double delta) {
   constexpr int BM = TL::BM, BN = TL::BN, LDA = TL::LDA, LDB = TL::LDB, MT = TL::MT, NT = TL::NT;
   constexpr int NTHREADS = TL::THREADS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -74,7 +83,8 @@ __global__ void __launch_bounds__(TL::THREADS, 512 / TL::THREADS)
   cplx* Bs = As + STAGES * BK * LDA;                    // [STAGES][BK][LDB]
 
   const GemmDesc d = descs[blockIdx.y];
-  const int tiles_m = (n + BM - 1) / BM;
+  const int kdim = sh.K;
+  const int tiles_m = (sh.M + BM - 1) / BM;
   const int m0 = (blockIdx.x % tiles_m) * BM;
   const int n0 = (blockIdx.x / tiles_m) * BN;
   const int tid = threadIdx.x;
@@ -97,14 +107,14 @@ __global__ void __launch_bounds__(TL::THREADS, 512 / TL::THREADS)
         // A tile: BM rows x 8 cols, consecutive threads -> consecutive rows.
         int r = idx % BM, k = idx / BM;
         int gr = m0 + r, gk = k0 + k;
-        bool va = (gr < n) && (gk < kdim);
-        cp_async16(as + k * LDA + r, va ? (const void*)(A + (size_t)gk * n + gr) : (const void*)A, va);
+        bool va = (gr < sh.M) && (gk < kdim);
+        cp_async16(as + k * LDA + r, va ? (const void*)(A + (size_t)gk * sh.lda + gr) : (const void*)A, va);
       } else {
-        // op(A)(r, k) = conj(A(k, r)), stored at A[r * n + k]: threads along k.
+        // op(A)(r, k) = conj(A(k, r)), stored at A[r * lda + k]: threads along k.
         int k = idx & 7, r = idx >> 3;
         int gr = m0 + r, gk = k0 + k;
-        bool va = (gr < n) && (gk < kdim);
-        cp_async16(as + k * LDA + r, va ? (const void*)(A + (size_t)gr * n + gk) : (const void*)A, va);
+        bool va = (gr < sh.M) && (gk < kdim);
+        cp_async16(as + k * LDA + r, va ? (const void*)(A + (size_t)gr * sh.lda + gk) : (const void*)A, va);
       }
     }
 #pragma unroll
@@ -114,14 +124,14 @@ __global__ void __launch_bounds__(TL::THREADS, 512 / TL::THREADS)
         // B tile: 8 rows x BN cols, consecutive threads -> consecutive k.
         int kb = idx & 7, c = idx >> 3;
         int gkb = k0 + kb, gc = n0 + c;
-        bool vb = (gkb < kdim) && (gc < n);
-        cp_async16(bs + kb * LDB + c, vb ? (const void*)(B + (size_t)gc * kdim + gkb) : (const void*)B, vb);
+        bool vb = (gkb < kdim) && (gc < sh.N);
+        cp_async16(bs + kb * LDB + c, vb ? (const void*)(B + (size_t)gc * sh.ldb + gkb) : (const void*)B, vb);
       } else {
-        // op(B)(k, c) = conj(B(c, k)), stored at B[k * n + c]: threads along c.
+        // op(B)(k, c) = conj(B(c, k)), stored at B[k * ldb + c]: threads along c.
         int c = idx % BN, kb = idx / BN;
         int gkb = k0 + kb, gc = n0 + c;
-        bool vb = (gkb < kdim) && (gc < n);
-        cp_async16(bs + kb * LDB + c, vb ? (const void*)(B + (size_t)gkb * n + gc) : (const void*)B, vb);
+        bool vb = (gkb < kdim) && (gc < sh.N);
+        cp_async16(bs + kb * LDB + c, vb ? (const void*)(B + (size_t)gkb * sh.ldb + gc) : (const void*)B, vb);
       }
     }
   };
@@ -188,13 +198,13 @@ __global__ void __launch_bounds__(TL::THREADS, 512 / TL::THREADS)
       for (int c = 0; c < 4; ++c) {
         int row = m0 + wm * (MT * 16) + mt * 16 + g + ((c >> 1) << 3);
         int col = n0 + wn * (NT * 8) + nt * 8 + tig * 2 + (c & 1);
-        if (row < n && col < n) {
+        if (row < sh.M && col < sh.N) {
           const double p1 = acc1[mt][nt][c], p2 = acc2[mt][nt][c];
           cplx v = mk(p1 - p2, acc3[mt][nt][c] - p1 - p2);
           v = cmul(alpha, v);
           if (d.rs) v = cmul(d.rs[row], v);
           if (d.cs) v = cmul(v, d.cs[col]);
-          size_t off = (size_t)col * n + row;
+          size_t off = (size_t)col * sh.ldc + row;
           if (d.Cin) v = cfma(beta, d.Cin[off], v);
           if (row == col) v.x += delta;
           d.C[off] = v;
@@ -203,17 +213,28 @@ __global__ void __launch_bounds__(TL::THREADS, 512 / TL::THREADS)
 }
 
 template <class TL>
-void launch_tile(const GemmDesc* d_descs, int batch, int n, cplx alpha, cplx beta, double delta,
-                 cudaStream_t stream, int kdim, int opA, int opB) {
+void launch_tile(const GemmDesc* d_descs, int batch, const GemmShape& sh, cplx alpha, cplx beta, double delta,
+                 cudaStream_t stream, int opA, int opB) {
   auto kern = opA ? (opB ? zgemm_kernel<TL, 1, 1> : zgemm_kernel<TL, 1, 0>)
                   : (opB ? zgemm_kernel<TL, 0, 1> : zgemm_kernel<TL, 0, 0>);
   ensure_smem((const void*)kern, TL::SMEM);
-  const int tiles = ((n + TL::BM - 1) / TL::BM) * ((n + TL::BN - 1) / TL::BN);
+  const int tiles = ((sh.M + TL::BM - 1) / TL::BM) * ((sh.N + TL::BN - 1) / TL::BN);
   for (int b0 = 0; b0 < batch; b0 += 65535) {
     int nb = batch - b0 < 65535 ? batch - b0 : 65535;
     dim3 grid(tiles, nb);
-    kern<<<grid, TL::THREADS, TL::SMEM, stream>>>(d_descs + b0, n, kdim, alpha, beta, delta);
+    kern<<<grid, TL::THREADS, TL::SMEM, stream>>>(d_descs + b0, sh, alpha, beta, delta);
   }
+}
+
+void launch(const GemmDesc* d_descs, int batch, const GemmShape& sh, cplx alpha, cplx beta, double delta,
+            cudaStream_t stream, int opA, int opB, int tile) {
+  if (tile != 32 && tile != 64) throw StatusError(ST_EINVAL, "GEMM tile must be 32 or 64");
+  if (batch <= 0 || sh.M <= 0 || sh.N <= 0) return;
+  if (tile == 32)
+    launch_tile<T32>(d_descs, batch, sh, alpha, beta, delta, stream, opA, opB);
+  else
+    launch_tile<T64>(d_descs, batch, sh, alpha, beta, delta, stream, opA, opB);
+  VRC_CUDA_CHECK(cudaGetLastError());
 }
 
 }  // namespace
@@ -222,13 +243,15 @@ void zgemm_batched(const GemmDesc* d_descs, int batch, int n, cplx alpha, cplx b
                    cudaStream_t stream, int kdim, int opA, int opB, int tile) {
   if (kdim < 0) kdim = n;
   if ((opA || opB) && kdim != n) throw StatusError(ST_EINVAL, "transposed GEMM operands must be square");
-  if (tile != 32 && tile != 64) throw StatusError(ST_EINVAL, "GEMM tile must be 32 or 64");
-  if (batch <= 0) return;
-  if (tile == 32)
-    launch_tile<T32>(d_descs, batch, n, alpha, beta, delta, stream, kdim, opA, opB);
-  else
-    launch_tile<T64>(d_descs, batch, n, alpha, beta, delta, stream, kdim, opA, opB);
-  VRC_CUDA_CHECK(cudaGetLastError());
+  launch(d_descs, batch, GemmShape{n, n, kdim, n, kdim, n}, alpha, beta, delta, stream, opA, opB, tile);
+}
+
+void zgemm_rect_batched(const GemmDesc* d_descs, int batch, int M, int N, int K, int lda, int ldb, int ldc,
+                        cplx alpha, cplx beta, cudaStream_t stream, int opA, int opB, int tile) {
+  if (K < 1 || lda < 1 || ldb < 1 || ldc < M) throw StatusError(ST_EINVAL, "invalid GEMM shape");
+  if ((opA ? lda < K : lda < M) || (opB ? ldb < N : ldb < K))
+    throw StatusError(ST_EINVAL, "GEMM leading dimension below the operand's rows");
+  launch(d_descs, batch, GemmShape{M, N, K, lda, ldb, ldc}, alpha, beta, 0.0, stream, opA, opB, tile);
 }
 
 }  // namespace vrc

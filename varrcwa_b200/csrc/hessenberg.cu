@@ -21,6 +21,8 @@
 // stored below the subdiagonal of the written-back matrix.
 #include <cooperative_groups.h>
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "householder.cuh"
 #include "kernels.h"
@@ -434,7 +436,257 @@ __global__ void __cluster_dims__(HC_CS, 1, 1) __launch_bounds__(HC_THREADS, 1)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Blocked reduction (the panel scheme of LAPACK's xGEHRD / xLAHR2, complex
+// form): for a panel of nb columns starting at column k, a panel kernel (one
+// CTA per matrix) forms the panel's reflectors v_i (tau_i), the triangular
+// factor T of H_k ... H_(k+nb-1) = I - V T V^H, and Y = A0 V T (A0 = the
+// matrix at the panel's start), finishing the panel's columns; the rest is
+// DMMA GEMMs:
+//   right update   A[:, k+nb:]   -= Y V[k+nb:, :]^H
+//   left update    A[J, k+nb:]   -= V[J, :] (T^H (V[J, :]^H A[J, k+nb:]))   (J = k+1 .. n-1)
+//   Q accumulation Q[:, J]       -= (Q[:, J] V[J, :]) T V[J, :]^H
+// In the panel, column j = k + i is first brought up to date with the
+// panel's previous reflectors -- from the right, c -= Y[:, :i] conj(V[j, :i]),
+// and from the left, c[J] -= V[:, :i] T[:i, :i]^H V[:, :i]^H c[J] -- then
+// reduced; Y[:, i] = tau_i (A0[:, j+1:] v_i - Y[:, :i] (V[:, :i]^H v_i)) and
+// T[:i, i] = -tau_i T[:i, :i] V[:, :i]^H v_i, T[i, i] = tau_i.  The only
+// pass over the trailing matrix per column is that product with A0, which
+// reads columns j+1 .. n-1, not yet written in this panel.
+constexpr int HB_NB = 32;
+constexpr int HB_THREADS = 256;
+constexpr int HB_WARPS = HB_THREADS / 32;
+
+struct HbLayout {
+  size_t V, Y, X, W, T, total;  // complex-element offsets in a matrix's scratch
+};
+__host__ __device__ inline HbLayout hb_layout(int n) {
+  HbLayout L;
+  size_t o = 0;
+  L.V = o;
+  o += (size_t)n * HB_NB;  // reflectors, column i = v_i (all n rows)
+  L.Y = o;
+  o += (size_t)n * HB_NB;
+  L.X = o;
+  o += (size_t)n * HB_NB;
+  L.W = o;
+  o += (size_t)HB_NB * n;  // V^H A, then T^H V^H A (leading dimension HB_NB)
+  L.T = o;
+  o += (size_t)HB_NB * HB_NB;
+  L.total = (o + 15) / 16 * 16;
+  return L;
+}
+
+template <int NT>
+__global__ void __launch_bounds__(HB_THREADS)
+    hb_panel_kernel(cplx* const* __restrict__ Hs, cplx* __restrict__ scratch, size_t stride, int n, int k, int nbp) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx* c = reinterpret_cast<cplx*>(smem_raw);  // [n] column being reduced
+  cplx* v = c + n;                              // [n] its reflector
+  __shared__ cplx s_w[HB_NB], s_w2[HB_NB], s_red[HB_WARPS];
+  __shared__ cplx s_tau, s_scale;
+  __shared__ double s_beta;
+  const HbLayout L = hb_layout(n);
+  cplx* H = Hs[blockIdx.x];
+  cplx* base = scratch + (size_t)blockIdx.x * stride;
+  cplx* V = base + L.V;
+  cplx* Y = base + L.Y;
+  cplx* T = base + L.T;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int J0 = k + 1;
+  // w[l] = sum_{r >= J0} conj(V[r, l]) x[r] for l < i (warp per l)
+  auto vh_dot = [&](const cplx* x, int i, cplx* w) {
+    for (int l = warp; l < i; l += HB_WARPS) {
+      const cplx* vl = V + (size_t)l * n;
+      cplx sacc = mk(0.0, 0.0);
+      for (int r = J0 + lane; r < n; r += 32) sacc = cadd(sacc, cmulc(vl[r], x[r]));
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        sacc.x += __shfl_xor_sync(0xffffffffu, sacc.x, o);
+        sacc.y += __shfl_xor_sync(0xffffffffu, sacc.y, o);
+      }
+      if (lane == 0) w[l] = sacc;
+    }
+  };
+  for (int i = 0; i < nbp; ++i) {
+    const int j = k + i;
+    // 1-2. column j, updated from the right by the panel's previous reflectors
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+      const int r = tid + HB_THREADS * t;
+      if (r < n) {
+        cplx a = H[(size_t)j * n + r];
+        for (int l = 0; l < i; ++l) a = csub(a, cmul(Y[(size_t)l * n + r], cconj(V[(size_t)l * n + j])));
+        c[r] = a;
+      }
+    }
+    __syncthreads();
+    // 3. and from the left: c[J] -= V T^H V^H c[J]
+    if (i > 0) {
+      vh_dot(c, i, s_w);
+      __syncthreads();
+      if (tid < i) {  // w2 = T^H w, T upper triangular (T(q, l) at T[l * HB_NB + q])
+        cplx a = mk(0.0, 0.0);
+        for (int q = 0; q <= tid; ++q) a = cadd(a, cmulc(T[(size_t)tid * HB_NB + q], s_w[q]));
+        s_w2[tid] = a;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int t = 0; t < NT; ++t) {
+        const int r = tid + HB_THREADS * t;
+        if (r >= J0 && r < n) {
+          cplx a = c[r];
+          for (int l = 0; l < i; ++l) a = csub(a, cmul(V[(size_t)l * n + r], s_w2[l]));
+          c[r] = a;
+        }
+      }
+      __syncthreads();
+    }
+    // 4. reflector from c[j+1 ..]
+    {
+      double part = 0.0;
+      for (int r = j + 2 + tid; r < n; r += HB_THREADS) part += cabs2(c[r]);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+      if (lane == 0) s_red[warp] = mk(part, 0.0);
+      __syncthreads();
+      if (tid == 0) {
+        double xn = 0.0;
+        for (int w = 0; w < HB_WARPS; ++w) xn += s_red[w].x;
+        double beta;
+        cplx tau, scale;
+        householder(c[j + 1], xn, &beta, &tau, &scale);
+        s_beta = beta;
+        s_tau = tau;
+        s_scale = scale;
+      }
+      __syncthreads();
+    }
+    const cplx tau = s_tau;
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+      const int r = tid + HB_THREADS * t;
+      if (r < n) {
+        cplx vr = mk(0.0, 0.0), hr = c[r];
+        if (r == j + 1) {
+          vr = mk(1.0, 0.0);
+          hr = mk(s_beta, 0.0);
+        } else if (r > j + 1) {
+          vr = cmul(c[r], s_scale);
+          hr = mk(0.0, 0.0);
+        }
+        v[r] = vr;
+        V[(size_t)i * n + r] = vr;
+        H[(size_t)j * n + r] = hr;  // column j is final
+      }
+    }
+    __syncthreads();
+    // 5. y = A0[:, j+1:] v (columns right of j are untouched in this panel)
+    cplx y[NT];
+#pragma unroll
+    for (int t = 0; t < NT; ++t) y[t] = mk(0.0, 0.0);
+    if (!(tau.x == 0.0 && tau.y == 0.0)) {
+      for (int col = j + 1; col < n; ++col) {
+        const cplx vc = v[col];
+        const cplx* hc = H + (size_t)col * n;
+#pragma unroll
+        for (int t = 0; t < NT; ++t) {
+          const int r = tid + HB_THREADS * t;
+          if (r < n) y[t] = cfma(hc[r], vc, y[t]);
+        }
+      }
+    }
+    // 6. Y[:, i] = tau (y - Y[:, :i] w'), w' = V[:, :i]^H v; T column i
+    if (i > 0) vh_dot(v, i, s_w);
+    __syncthreads();
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+      const int r = tid + HB_THREADS * t;
+      if (r < n) {
+        cplx a = y[t];
+        for (int l = 0; l < i; ++l) a = csub(a, cmul(Y[(size_t)l * n + r], s_w[l]));
+        Y[(size_t)i * n + r] = cmul(tau, a);
+      }
+    }
+    if (tid <= i) {
+      cplx a = tau;
+      if (tid < i) {  // T(q, i) = -tau sum_{p = q}^{i-1} T(q, p) w'[p]
+        a = mk(0.0, 0.0);
+        for (int p = tid; p < i; ++p) a = cadd(a, cmul(T[(size_t)p * HB_NB + tid], s_w[p]));
+        a = cneg(cmul(tau, a));
+      }
+      T[(size_t)i * HB_NB + tid] = a;
+    }
+    __syncthreads();
+  }
+}
+
+// GEMM descriptors of one panel's seven products for every matrix (stage s
+// at descs + s * batch): right update, V^H A, T^H (.), left update, Q V, (.) T,
+// Q update.
+__global__ void hb_desc_kernel(cplx* const* __restrict__ Hs, cplx* const* __restrict__ Zs, cplx* __restrict__ scratch,
+                               size_t stride, int n, int k, int nbp, int batch, GemmDesc* __restrict__ descs) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= batch) return;
+  const HbLayout L = hb_layout(n);
+  cplx* H = Hs[b];
+  cplx* Z = Zs[b];
+  cplx* base = scratch + (size_t)b * stride;
+  cplx *V = base + L.V, *Y = base + L.Y, *X = base + L.X, *W = base + L.W, *T = base + L.T;
+  const int J0 = k + 1, c0 = k + nbp;
+  cplx* Hr = H + (size_t)c0 * n;  // columns right of the panel
+  descs[0 * batch + b] = {Y, V + c0, Hr, Hr, nullptr, nullptr};            // Hr -= Y V[c0:]^H
+  descs[1 * batch + b] = {V + J0, Hr + J0, W, nullptr, nullptr, nullptr};  // W = V[J]^H Hr[J]
+  descs[2 * batch + b] = {T, W, X, nullptr, nullptr, nullptr};             // X = T^H W
+  descs[3 * batch + b] = {V + J0, X, Hr + J0, Hr + J0, nullptr, nullptr};  // Hr[J] -= V[J] X
+  descs[4 * batch + b] = {Z + (size_t)J0 * n, V + J0, X, nullptr, nullptr, nullptr};  // X = Z[:, J] V[J]
+  descs[5 * batch + b] = {X, T, Y, nullptr, nullptr, nullptr};                      // Y = X T
+  descs[6 * batch + b] = {Y, V + J0, Z + (size_t)J0 * n, Z + (size_t)J0 * n, nullptr, nullptr};  // Z[:, J] -= Y V[J]^H
+}
+
+template <int NT>
+void launch_hb_panel(cplx* const* H, cplx* scratch, size_t stride, int batch, int n, int k, int nbp, cudaStream_t st) {
+  const size_t smem = 2 * (size_t)n * sizeof(cplx);
+  ensure_smem((const void*)hb_panel_kernel<NT>, smem);
+  hb_panel_kernel<NT><<<batch, HB_THREADS, smem, st>>>(H, scratch, stride, n, k, nbp);
+}
+
 }  // namespace
+
+size_t hessenberg_blocked_scratch(int n) { return hb_layout(n).total * sizeof(cplx); }
+size_t hessenberg_blocked_descs(int batch) { return 7 * (size_t)batch * sizeof(GemmDesc); }
+
+void hessenberg_blocked_batched(cplx* const* d_H, cplx* const* d_Z, int batch, int n, void* scratch,
+                                size_t stride_bytes, void* descs, cudaStream_t st) {
+  if (batch <= 0) return;
+  if (n < 3 || n > 1024 || batch > 65535) throw StatusError(ST_EINVAL, "blocked Hessenberg: n in [3, 1024]");
+  if (stride_bytes < hessenberg_blocked_scratch(n) || stride_bytes % sizeof(cplx))
+    throw StatusError(ST_EINVAL, "blocked Hessenberg: scratch stride below its layout");
+  const size_t stride = stride_bytes / sizeof(cplx);
+  cplx* scr = static_cast<cplx*>(scratch);
+  GemmDesc* dd = static_cast<GemmDesc*>(descs);
+  set_identity_batched(d_Z, batch, n, 1.0, st);
+  const cplx one = mk(1.0, 0.0), mone = mk(-1.0, 0.0), zero = mk(0.0, 0.0);
+  for (int k = 0; k < n - 2; k += HB_NB) {
+    const int nbp = std::min(HB_NB, n - 2 - k);
+    const int J0 = k + 1, MJ = n - J0, c0 = k + nbp, N2 = n - c0;
+    if (n <= 256) launch_hb_panel<1>(d_H, scr, stride, batch, n, k, nbp, st);
+    else if (n <= 512) launch_hb_panel<2>(d_H, scr, stride, batch, n, k, nbp, st);
+    else launch_hb_panel<4>(d_H, scr, stride, batch, n, k, nbp, st);
+    VRC_CUDA_CHECK(cudaGetLastError());
+    hb_desc_kernel<<<(batch + 127) / 128, 128, 0, st>>>(d_H, d_Z, scr, stride, n, k, nbp, batch, dd);
+    VRC_CUDA_CHECK(cudaGetLastError());
+    if (N2 > 0) {
+      zgemm_rect_batched(dd + 0 * (size_t)batch, batch, n, N2, nbp, n, n, n, mone, one, st, 0, 1);
+      zgemm_rect_batched(dd + 1 * (size_t)batch, batch, nbp, N2, MJ, n, n, HB_NB, one, zero, st, 1, 0);
+      zgemm_rect_batched(dd + 2 * (size_t)batch, batch, nbp, N2, nbp, HB_NB, HB_NB, HB_NB, one, zero, st, 1, 0);
+      zgemm_rect_batched(dd + 3 * (size_t)batch, batch, MJ, N2, nbp, n, HB_NB, n, mone, one, st, 0, 0);
+    }
+    zgemm_rect_batched(dd + 4 * (size_t)batch, batch, n, nbp, MJ, n, n, n, one, zero, st, 0, 0);
+    zgemm_rect_batched(dd + 5 * (size_t)batch, batch, n, nbp, nbp, n, HB_NB, n, one, zero, st, 0, 0);
+    zgemm_rect_batched(dd + 6 * (size_t)batch, batch, n, MJ, nbp, n, n, n, mone, one, st, 0, 1);
+  }
+}
 
 bool hessenberg_cluster_fits(int n) { return n >= 3 && n <= HG_MAXN; }
 

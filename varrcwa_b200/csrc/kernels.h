@@ -24,6 +24,12 @@ struct GemmDesc {
 // tile: 64 (64 x 64 complex per CTA) or 32 (32 x 32); results are identical.
 void zgemm_batched(const GemmDesc* d_descs, int batch, int n, cplx alpha, cplx beta, double delta,
                    cudaStream_t stream, int kdim = -1, int opA = 0, int opB = 0, int tile = 64);  // kdim < 0: n
+// Rectangular form: C (M x N, leading dimension ldc) = alpha op(A) op(B)
+// (+ beta Cin, same ldc) with op(A) M x K and op(B) K x N; A is stored M x K
+// (lda) or, with opA, K x M; B is stored K x N (ldb) or, with opB, N x K.
+// The descriptors' rs / cs scale rows (M) / columns (N).
+void zgemm_rect_batched(const GemmDesc* d_descs, int batch, int M, int N, int K, int lda, int ldb, int ldc,
+                        cplx alpha, cplx beta, cudaStream_t stream, int opA = 0, int opB = 0, int tile = 64);
 
 // ---- inverse (in place) -------------------------------------------------------
 int zinv_panel_width(int n);
@@ -43,6 +49,14 @@ void hessenberg_batched(cplx* const* d_H, cplx* const* d_Z, int batch, int n, cu
 // distributed shared memory (hessenberg.cu); for n where it fits.
 bool hessenberg_cluster_fits(int n);
 void hessenberg_cluster_batched(cplx* const* d_H, cplx* const* d_Z, int batch, int n, cudaStream_t st);
+// Blocked reduction (32-column panels, DMMA GEMM updates): scratch of
+// hessenberg_blocked_scratch(n) bytes per matrix (matrix b's at scratch +
+// b * stride_bytes) and a device buffer of hessenberg_blocked_descs(batch)
+// bytes for the GEMM descriptors; batch <= 65535.
+size_t hessenberg_blocked_scratch(int n);
+size_t hessenberg_blocked_descs(int batch);
+void hessenberg_blocked_batched(cplx* const* d_H, cplx* const* d_Z, int batch, int n, void* scratch,
+                                size_t stride_bytes, void* descs, cudaStream_t st);
 // Complex Schur form + Schur vectors.  d_logs: one rotation-log buffer of
 // schur_log_bytes(n) bytes per matrix (device scratch, contents overwritten).
 // parts: SCHUR_ITERATE (QR sweeps on the active windows, rotations logged),
