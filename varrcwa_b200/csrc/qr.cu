@@ -177,17 +177,25 @@ __device__ __forceinline__ void rotate2(cplx& a, cplx& b, cplx tau, cplx v2) {
 // Carries one value down a chain of cnt rotations on consecutive index
 // pairs (k0, k0+1), (k0+1, k0+2), ...: row transforms on a column (rowop,
 // entries p0[t], stride 1) or column transforms on a row (stride n).  The
-// entries are fetched eight at a time ahead of use.
+// entries are fetched in groups of CG, double buffered: the loads of the
+// next group are issued before the current group's rotations, so their
+// latency overlaps the arithmetic.  Every entry a rotation writes lies below
+// the next group's (the chain moves forward), so the early loads read
+// values no rotation of this chain changes.
+constexpr int CG = 4;
 __device__ __forceinline__ void carry_chain(cplx* p0, size_t stride, int cnt, const cplx* taus, const cplx* v2s,
                                             bool rowop) {
   cplx c = p0[0];
-  for (int t0 = 0; t0 < cnt; t0 += 8) {
-    cplx q[8];
+  cplx q[CG], qn[CG];
 #pragma unroll
-    for (int u = 0; u < 8; ++u)
-      if (t0 + u < cnt) q[u] = p0[(size_t)(t0 + u + 1) * stride];
+  for (int u = 0; u < CG; ++u)
+    if (u < cnt) q[u] = p0[(size_t)(u + 1) * stride];
+  for (int t0 = 0; t0 < cnt; t0 += CG) {
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
+    for (int u = 0; u < CG; ++u)
+      if (t0 + CG + u < cnt) qn[u] = p0[(size_t)(t0 + CG + u + 1) * stride];
+#pragma unroll
+    for (int u = 0; u < CG; ++u) {
       if (t0 + u < cnt) {
         cplx b = q[u];
         if (rowop)
@@ -198,6 +206,8 @@ __device__ __forceinline__ void carry_chain(cplx* p0, size_t stride, int cnt, co
         c = b;
       }
     }
+#pragma unroll
+    for (int u = 0; u < CG; ++u) q[u] = qn[u];
   }
   p0[(size_t)cnt * stride] = c;
 }
