@@ -581,20 +581,42 @@ __global__ void __launch_bounds__(HB_THREADS)
       }
     }
     __syncthreads();
-    // 5. y = A0[:, j+1:] v (columns right of j are untouched in this panel)
+    // 5. y = A0[:, j+1:] v (columns right of j are untouched in this panel);
+    // four partial sums over interleaved columns keep four independent FMA
+    // chains (and their loads) in flight, added in a fixed order
     cplx y[NT];
+    {
+      cplx ya[4][NT];
 #pragma unroll
-    for (int t = 0; t < NT; ++t) y[t] = mk(0.0, 0.0);
-    if (!(tau.x == 0.0 && tau.y == 0.0)) {
-      for (int col = j + 1; col < n; ++col) {
-        const cplx vc = v[col];
-        const cplx* hc = H + (size_t)col * n;
+      for (int u = 0; u < 4; ++u)
 #pragma unroll
-        for (int t = 0; t < NT; ++t) {
-          const int r = tid + HB_THREADS * t;
-          if (r < n) y[t] = cfma(hc[r], vc, y[t]);
+        for (int t = 0; t < NT; ++t) ya[u][t] = mk(0.0, 0.0);
+      if (!(tau.x == 0.0 && tau.y == 0.0)) {
+        int col = j + 1;
+        for (; col + 3 < n; col += 4) {
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const cplx vc = v[col + u];
+            const cplx* hc = H + (size_t)(col + u) * n;
+#pragma unroll
+            for (int t = 0; t < NT; ++t) {
+              const int r = tid + HB_THREADS * t;
+              if (r < n) ya[u][t] = cfma(hc[r], vc, ya[u][t]);
+            }
+          }
+        }
+        for (; col < n; ++col) {
+          const cplx vc = v[col];
+          const cplx* hc = H + (size_t)col * n;
+#pragma unroll
+          for (int t = 0; t < NT; ++t) {
+            const int r = tid + HB_THREADS * t;
+            if (r < n) ya[0][t] = cfma(hc[r], vc, ya[0][t]);
+          }
         }
       }
+#pragma unroll
+      for (int t = 0; t < NT; ++t) y[t] = cadd(cadd(ya[0][t], ya[1][t]), cadd(ya[2][t], ya[3][t]));
     }
     // 6. Y[:, i] = tau (y - Y[:, :i] w'), w' = V[:, :i]^H v; T column i
     if (i > 0) vh_dot(v, i, s_w);

@@ -24,6 +24,8 @@
 // Deflation: small subdiagonals (Ahues-Tisseur test) split the window;
 // exceptional shifts at iterations 10 and 20; at most 30*max(10,n)
 // iterations per eigenvalue and 30n+300 in total, else ST_ENOCONV.
+#include <cstdlib>
+
 #include "common.cuh"
 #include "householder.cuh"
 #include "kernels.h"
@@ -182,7 +184,7 @@ __device__ __forceinline__ void rotate2(cplx& a, cplx& b, cplx tau, cplx v2) {
 // latency overlaps the arithmetic.  Every entry a rotation writes lies below
 // the next group's (the chain moves forward), so the early loads read
 // values no rotation of this chain changes.
-constexpr int CG = 4;
+template <int CG>
 __device__ __forceinline__ void carry_chain(cplx* p0, size_t stride, int cnt, const cplx* taus, const cplx* v2s,
                                             bool rowop) {
   cplx c = p0[0];
@@ -212,7 +214,10 @@ __device__ __forceinline__ void carry_chain(cplx* p0, size_t stride, int cnt, co
   p0[(size_t)cnt * stride] = c;
 }
 
-__global__ void __launch_bounds__(QR_THREADS, 2)
+// MINB: resident CTAs per SM the registers are sized for; with three the
+// carry chains prefetch two entries instead of four (no spills either way).
+template <int MINB>
+__global__ void __launch_bounds__(QR_THREADS, MINB)
     hqr_kernel(cplx* const* __restrict__ Hs, void* const* __restrict__ logs, cplx* const* __restrict__ Ws, int n,
                int sweep_cap, long long rot_cap, int* __restrict__ status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -422,7 +427,7 @@ __global__ void __launch_bounds__(QR_THREADS, 2)
             if (ra1 <= ra0) continue;
             const int k0 = m + ra0 - 3 * b;
             cplx* p0 = rowop ? H + (size_t)(de + 1 + task) * n + k0 : H + (size_t)k0 * n + (m + task - nright);
-            carry_chain(p0, rowop ? 1 : (size_t)n, ra1 - ra0, s_tau + b * QB + (ra0 - r0), s_v2 + b * QB + (ra0 - r0),
+            carry_chain<(MINB >= 3 ? 2 : 4)>(p0, rowop ? 1 : (size_t)n, ra1 - ra0, s_tau + b * QB + (ra0 - r0), s_v2 + b * QB + (ra0 - r0),
                         rowop);
           }
         }
@@ -630,7 +635,14 @@ __global__ void __launch_bounds__(RP_THREADS, 4)
 void schur_batched(cplx* const* d_H, cplx* const* d_Z, cplx* const* d_W, void* const* d_logs, int batch, int n,
                    int* d_status, cudaStream_t st, int parts) {
   if (batch <= 0) return;
-  ensure_smem((const void*)hqr_kernel, QR_SMEM);
+  // resident Schur CTAs per SM: 2 (default) or 3 (VRC_QR_CTAS=3); the
+  // arithmetic is the same, only the registers and the prefetch depth differ
+  static const int minb = [] {
+    const char* e = std::getenv("VRC_QR_CTAS");
+    return (e && std::atoi(e) == 3) ? 3 : 2;
+  }();
+  auto hqr = minb == 3 ? hqr_kernel<3> : hqr_kernel<2>;
+  ensure_smem((const void*)hqr, QR_SMEM);
   ensure_smem((const void*)qr_replay_rows_kernel, RP_SMEM);
   ensure_smem((const void*)qr_replay_cols_kernel, RP_SMEM);
   const int cc = schur_sweep_cap(n);
@@ -640,7 +652,7 @@ void schur_batched(cplx* const* d_H, cplx* const* d_Z, cplx* const* d_W, void* c
   for (int b0 = 0; b0 < batch; b0 += 65535) {
     const int nb = min(65535, batch - b0);
     if (parts & SCHUR_ITERATE)
-      hqr_kernel<<<nb, QR_THREADS, QR_SMEM, st>>>(d_H + b0, d_logs + b0, d_W + b0, n, cc, rc,
+      hqr<<<nb, QR_THREADS, QR_SMEM, st>>>(d_H + b0, d_logs + b0, d_W + b0, n, cc, rc,
                                                   d_status ? d_status + b0 : nullptr);
     if (parts & SCHUR_REPLAY) {
       qr_replay_rows_kernel<<<dim3(2 * row_blocks, nb), RP_THREADS, rp_smem, st>>>(d_H + b0, d_Z + b0, d_logs + b0,
