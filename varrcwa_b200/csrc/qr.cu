@@ -6,9 +6,15 @@
 // trailing nb x nb block; one Wilkinson or exceptional shift when nb = 1):
 // bulge a (warp a) is introduced at round 3a and moves one position per
 // round, so in round r it performs step k = m + r - 3a.  Bulges three apart
-// use reflectors on disjoint index pairs, which commute: every round applies
-// all row transforms, synchronises, then all column transforms together with
-// each bulge's next reflector.  Rounds run in chunks of QB inside a diagonal
+// use reflectors on disjoint index pairs.  In a round every entry receives at
+// most one row transform (L) and one column transform (R), and L (X R) =
+// (L X) R, so the warps need not wait for one another inside a round: the
+// only entries two warps share are the 2 x 2 blocks where a bulge's rows
+// cross a leading bulge's columns, and the row-transforming warp applies both
+// there (L first, then R, as a row phase followed by a column phase would),
+// while the leading bulge's column transform skips those rows.  Each warp
+// then forms its bulge's next reflector, and one CTA barrier ends the round.
+// Rounds run in chunks of QB inside a diagonal
 // window D held in shared memory; after a chunk the rest of the active
 // window is updated by one thread per row or column, which carries a value
 // down each bulge's chain of the chunk (carry_chain).  Rows above the
@@ -372,29 +378,48 @@ __global__ void __launch_bounds__(QR_THREADS, MINB)
         for (int r = r0; r < r1; ++r) {
           const int k = m + r - 3 * a;
           const bool act = mine && k >= m && k <= i - 1;
-          cplx tau = mk(0.0, 0.0), v2 = mk(0.0, 0.0);
           if (act) {
-            tau = s_tau[a * QB + (r - r0)];
-            v2 = s_v2[a * QB + (r - r0)];
-            // phase 1: row transform of rows k, k+1 over columns k..de
-            const cplx tauc = cconj(tau), v2c = cconj(v2);
-            for (int j = k + lane; j <= de; j += 32) {
-              const cplx x = dd(k, j), y = dd(k + 1, j);
-              const cplx s = cmul(tauc, cadd(x, cmul(v2c, y)));
-              dd(k, j) = csub(x, s);
-              dd(k + 1, j) = csub(y, cmul(s, v2));
+            const cplx tau = s_tau[a * QB + (r - r0)], v2 = s_v2[a * QB + (r - r0)];
+            // row transform of rows k, k+1 over columns k..de
+            {
+              const cplx tauc = cconj(tau), v2c = cconj(v2);
+              for (int j = k + lane; j <= de; j += 32) {
+                const cplx x = dd(k, j), y = dd(k + 1, j);
+                const cplx s = cmul(tauc, cadd(x, cmul(v2c, y)));
+                dd(k, j) = csub(x, s);
+                dd(k + 1, j) = csub(y, cmul(s, v2));
+              }
             }
-          }
-          __syncthreads();
-          if (act) {
-            // phase 2: column transform of columns k, k+1 over rows ds..min(k+2, i)
-            const cplx v2c = cconj(v2);
-            const int re = min(k + 2, i);
-            for (int rr = ds + lane; rr <= re; rr += 32) {
-              const cplx p = dd(rr, k), q = dd(rr, k + 1);
-              const cplx s = cmul(tau, cadd(p, cmul(v2, q)));
-              dd(rr, k) = csub(p, s);
-              dd(rr, k + 1) = csub(q, cmul(s, v2c));
+            __syncwarp();
+            // the leading bulges' column transforms on rows k, k+1: bulge
+            // b = a - 1 - lane acts on columns kb, kb + 1, kb = k + 3 (a - b)
+            {
+              const int b = a - 1 - lane, kb = k + 3 * (lane + 1);
+              if (b >= 0 && kb <= i - 1) {
+                const cplx tb = s_tau[b * QB + (r - r0)], vb = s_v2[b * QB + (r - r0)], vbc = cconj(vb);
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                  const cplx p = dd(k + q, kb), w = dd(k + q, kb + 1);
+                  const cplx s = cmul(tb, cadd(p, cmul(vb, w)));
+                  dd(k + q, kb) = csub(p, s);
+                  dd(k + q, kb + 1) = csub(w, cmul(s, vbc));
+                }
+              }
+            }
+            // column transform of columns k, k+1 over rows ds..min(k+2, i),
+            // except the rows of the trailing bulges (bulge a + q on rows
+            // k - 3q, k - 3q + 1), which their own warps transform
+            {
+              const cplx v2c = cconj(v2);
+              const int re = min(k + 2, i);
+              for (int rr = ds + lane; rr <= re; rr += 32) {
+                const int dk = k - rr, q = (dk + 1) / 3;
+                if (dk >= 2 && dk % 3 != 1 && a + q < nb && k - 3 * q >= m) continue;
+                const cplx p = dd(rr, k), w = dd(rr, k + 1);
+                const cplx s = cmul(tau, cadd(p, cmul(v2, w)));
+                dd(rr, k) = csub(p, s);
+                dd(rr, k + 1) = csub(w, cmul(s, v2c));
+              }
             }
           }
           __syncwarp();
