@@ -73,3 +73,25 @@ def test_zgemm_tiles_identical(ctx, n, monkeypatch):
         out[tile] = ctx.zgemm(A, B)
     assert np.array_equal(out["64"], out["32"])
     assert relerr(out["32"], A @ B) < 1e-14
+
+
+@pytest.mark.parametrize("mode", ["2", "1"])
+def test_gemm_bulk_staging_bit_identical(ctx, mode, monkeypatch):
+    """The 64 x 64 tile with its operands staged by bulk copies
+    (VRC_GEMM_BULK=2: two CTAs per SM, 1: one) computes the same products bit
+    for bit as the 16-byte cp.async staging: square products with ragged
+    edges (n = 242 = 3 x 64 + 50, k = 30 x 8 + 2), and the eigensolver, whose
+    blocked Hessenberg reduction multiplies rectangular and conjugate-
+    transposed operands."""
+    A, B = _rand(16, 242), _rand(16, 242)
+    E = _rand(3, 242)
+    monkeypatch.setenv("VRC_GEMM_TILE", "64")
+    monkeypatch.delenv("VRC_GEMM_BULK", raising=False)
+    ref = ctx.zgemm(A, B)
+    lam0, W0 = ctx.eig(E)
+    monkeypatch.setenv("VRC_GEMM_BULK", mode)
+    out = ctx.zgemm(A, B)
+    lam1, W1 = ctx.eig(E)
+    assert np.array_equal(out, ref)
+    assert relerr(out, A @ B) < 1e-14
+    assert np.array_equal(lam1, lam0) and np.array_equal(W1, W0)

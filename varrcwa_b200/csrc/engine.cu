@@ -204,6 +204,7 @@ static double host_now_ms() {
 void Engine::sync() {
   const double t0 = host_now_ms();
   VRC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+  gemm_bulk_check();
   t_sync_ret_ = host_now_ms();
   sync_ms_ += t_sync_ret_ - t0;
   ++nsync_;

@@ -22,6 +22,9 @@ struct GemmDesc {
 };
 // opA / opB = 1 takes that operand as its conjugate transpose (kdim == n).
 // tile: 64 (64 x 64 complex per CTA) or 32 (32 x 32); results are identical.
+// throws ST_ETIMEOUT when a bulk-staged GEMM (VRC_GEMM_BULK) gave up waiting
+// for a stage since the last check; call after a stream synchronisation
+void gemm_bulk_check();
 void zgemm_batched(const GemmDesc* d_descs, int batch, int n, cplx alpha, cplx beta, double delta,
                    cudaStream_t stream, int kdim = -1, int opA = 0, int opB = 0, int tile = 64);  // kdim < 0: n
 // Rectangular form: C (M x N, leading dimension ldc) = alpha op(A) op(B)
