@@ -396,7 +396,7 @@ def rule_weights(zs, z, spline=False):
     return np.array([ev(zs, np.eye(K)[k], z) for k in range(K)])
 
 
-def knot_gradient(desc, cuts, gS, gW0=None, gV0=None, gW1=None, gV1=None, h=1e-6):
+def knot_gradient(desc, cuts, gS, gW0=None, gV0=None, gW1=None, gV1=None, h=1e-6, fw=None):
     """dL/d(knot values) of every coordinate rule of a grid cell (x rules
     first, then y rules, each rule's knots in order), for cotangents gS of the
     final blocks and optional explicit cotangents of the end bases: the
@@ -408,10 +408,12 @@ def knot_gradient(desc, cuts, gS, gW0=None, gV0=None, gW1=None, gV1=None, h=1e-6
     z0 and z1 (eig_adjoint).  At every node each moving coordinate's
     dP/dx, dQ/dx is a central difference of the sampler (+-h on that
     coordinate alone), contracted to dL/dx(z) and spread over the rule's knots
-    by d x(z) / d vals."""
+    by d x(z) / d vals.  fw: the forward replay on these cuts when the caller
+    already has it (segments_forward of the same cell)."""
     from .structures_adapter import make_sampler
     s = make_sampler(desc)
-    fw = segments_forward(s, cuts)
+    if fw is None:
+        fw = segments_forward(s, cuts)
     gsegs, gfirst = segments_block_adjoints(fw, gS, want_first=True)
     spline = bool(desc.get("spline"))
     rules = [(0, r) for r in desc.get("xrules", [])] + [(1, r) for r in desc.get("yrules", [])]
