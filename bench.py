@@ -64,6 +64,11 @@ def parse():
                    help="cells timed one per call (the plain per-solve form of the metric); 0 skips")
     p.add_argument("--no-sub", action="store_true", help="skip the c2 and forward+adjoint sub-lines")
     p.add_argument("--orders", type=int, default=9, help="c4: harmonics per axis (9 = config 4, 15 = 15x15 orders)")
+    p.add_argument("--kernel", default=None, choices=["zgemm", "eig", "assembly"],
+                   help="time one kernel entry of the C ABI instead of a workload, for kernel profiles: vrc_zgemm "
+                        "or vrc_eig on seeded random n x n matrices (--n, --batch), or vrc_sample_pq on --batch "
+                        "z samples of a config-2 pillar cell (11x11 orders, 256x256 raster)")
+    p.add_argument("--n", type=int, default=242, help="--kernel: matrix order")
     a = p.parse_args()
     if a.pe is None:
         a.pe = 1e-6 if a.workload == "c1" else 1e-2
@@ -638,6 +643,54 @@ def measure_c5(ctx, orders=21, batch=2, steps=1, length=20.0, ncontrol=64):
                        "output": "mode-conversion power and its gradient w.r.t. every control point"}}
 
 
+def run_kernel(a):
+    """One C-ABI kernel entry (vrc_zgemm: batch products of n x n complex
+    matrices; vrc_eig: batch eigen-decompositions) on seeded random inputs:
+    --warmup untimed calls, then --steps timed ones; device time per call and
+    the family's busy time and rate from the engine's counters."""
+    import numpy as np
+    from varrcwa_b200.capi import Context
+    ctx = Context(0)
+    n, b = a.n, a.batch
+    if a.kernel == "assembly":
+        from varrcwa_b200 import structures as st
+        cell = st.pillar_config2(seed=2000, npix=a.npix)
+        n = 2 * cell["nx"] * cell["ny"]
+        zs = np.linspace(cell["z0"], cell["z1"], b)
+        call = lambda: ctx.sample_pq(cell, zs)
+    else:
+        rng = np.random.default_rng(7)
+        A = rng.standard_normal((b, n, n)) + 1j * rng.standard_normal((b, n, n))
+        B = rng.standard_normal((b, n, n)) + 1j * rng.standard_normal((b, n, n))
+        call = (lambda: ctx.zgemm(A, B)) if a.kernel == "zgemm" else (lambda: ctx.eig(A))
+    for _ in range(a.warmup):
+        call()
+    ctx.set_profiling(True)
+    ms = []
+    for _ in range(a.steps):
+        call()
+        ms.append(ctx.timing()["device_ms"])
+    stats = ctx.kernel_stats()
+    ctx.set_profiling(False)
+    line = {"kernel": a.kernel, "n": n, "batch": b, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_call": sum(ms) / len(ms), "kernel_breakdown": breakdown_of(stats)}
+    if a.kernel == "assembly":
+        # algorithmic bytes per sample: the eps raster in, fe11, fe22, fe33 and P, Q out
+        m = n // 2
+        per = 16.0 * (a.npix * a.npix + 3 * m * m + 2 * n * n)
+        line["algorithmic_bytes_per_sample"] = per
+        fam = stats.get("assembly")
+        if fam:  # the assembly family's own busy time, without the copies of P, Q to the host
+            busy = _busy(fam) / a.steps
+            line["assembly_ms_per_call"] = busy
+            line["achieved_gbs"] = per * b / (busy * 1e-3) / 1e9
+    else:
+        flops = (8.0 if a.kernel == "zgemm" else 80.0) * n ** 3 * b
+        line["nominal_tflops"] = flops / (line["ms_per_call"] * 1e-3) / 1e12
+        line["nominal_flops"] = "8 n^3 per product" if a.kernel == "zgemm" else "80 n^3 per decomposition"
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -656,6 +709,9 @@ def main():
         sys.exit(subprocess.call(cmd))
     if world != a.gpus:
         sys.exit(f"bench.py: --gpus {a.gpus} but WORLD_SIZE={world}: launch one process per GPU")
+    if a.kernel:
+        run_kernel(a)
+        return
     if a.impl == "reference":
         run_reference(a, rank, world)
         return

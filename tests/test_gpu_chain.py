@@ -49,7 +49,11 @@ def test_chain_matches_oracle_blocks_powers_and_fields(ctx):
     for pol, (px, py) in enumerate(((1.0, 0.0), (0.0, 1.0))):
         R, Tr = O.order_powers(T, s0, ds[-1]["end1"], ds[0]["end0"], px, py, side="top")
         assert relerr(p["R"][pol], R) < TOL and relerr(p["T"][pol], Tr) < TOL
-        assert abs(p["R"][pol].sum() + p["T"][pol].sum() - 1.0) < 1e-10
+        # perturbative varRCWA sections (pe = 1e-2) conserve flux only to the
+        # method's accuracy, the same for the oracle; stacks of z-uniform
+        # sections conserve it to 1e-10 (test_oracle_chain.py)
+        assert abs(p["R"][pol].sum() + p["T"][pol].sum() - (R.sum() + Tr.sum())) < 1e-9
+        assert abs(p["R"][pol].sum() + p["T"][pol].sum() - 1.0) < 1e-3
     # interface fields for an incident entrance mode: the transverse E field
     # on a grid over the period does not depend on any basis choice
     n = r["W0"].shape[0]

@@ -175,7 +175,7 @@ Engine::Engine(int device) : device_(device) {
   VRC_CUDA_CHECK(cudaSetDevice(device));
   VRC_CUDA_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   own_stream_ = true;
-  stage_cap_ = (size_t)64 << 20;
+  stage_cap_ = (size_t)128 << 20;  // two halves of 64 MB
   VRC_CUDA_CHECK(cudaMallocHost(&h_stage_, stage_cap_));
   VRC_CUDA_CHECK(cudaMalloc(&d_stage_, stage_cap_));
 }
@@ -307,13 +307,24 @@ void Engine::free_bytes(void* p, size_t b) {
   if (p) pool((b + 255) / 256 * 256).put(p);
 }
 
+// Launch arguments (descriptor and pointer arrays) are staged in two halves
+// of a pinned ring.  When the current half is full the engine synchronises
+// and continues in the other half, so arguments already staged for the
+// launch being prepared (the earlier operands of one call) stay intact; the
+// half they sit in is reused only after the next synchronisation.
 void* Engine::stage(const void* data, size_t nbytes) {
-  size_t need = (nbytes + 255) / 256 * 256;
-  if (need > stage_cap_) throw StatusError(ST_EINVAL, "descriptor batch too large");
-  if (stage_off_ + need > stage_cap_) sync();
-  std::memcpy(h_stage_ + stage_off_, data, nbytes);
-  void* d = d_stage_ + stage_off_;
-  VRC_CUDA_CHECK(cudaMemcpyAsync(d, h_stage_ + stage_off_, nbytes, cudaMemcpyHostToDevice, stream_));
+  const size_t need = (nbytes + 255) / 256 * 256;
+  const size_t half = stage_cap_ / 2;
+  if (need > half) throw StatusError(ST_EINVAL, "descriptor batch too large");
+  if (stage_off_ + need > half) {
+    const int next = stage_half_ ^ 1;
+    sync();  // every launch so far has completed: both halves are free
+    stage_half_ = next;
+  }
+  char* h = h_stage_ + stage_half_ * half + stage_off_;
+  char* d = d_stage_ + stage_half_ * half + stage_off_;
+  std::memcpy(h, data, nbytes);
+  VRC_CUDA_CHECK(cudaMemcpyAsync(d, h, nbytes, cudaMemcpyHostToDevice, stream_));
   stage_off_ += need;
   return d;
 }

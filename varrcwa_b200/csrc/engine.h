@@ -357,6 +357,7 @@ class Engine {
   char* h_stage_ = nullptr;
   char* d_stage_ = nullptr;
   size_t stage_cap_ = 0, stage_off_ = 0;
+  int stage_half_ = 0;  // the half of the staging ring in use
   void* ws_ = nullptr;
   size_t ws_cap_ = 0;
   // pinned staging of host-sampler matrices and the event of its last copy

@@ -638,6 +638,9 @@ __global__ void __launch_bounds__(HB_THREADS)
         a = cneg(cmul(tau, a));
       }
       T[(size_t)i * HB_NB + tid] = a;
+    } else if (tid < HB_NB) {
+      // the strictly lower part: the GEMM stages read T as a full block
+      T[(size_t)i * HB_NB + tid] = mk(0.0, 0.0);
     }
     __syncthreads();
   }

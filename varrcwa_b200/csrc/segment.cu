@@ -126,7 +126,7 @@ __global__ void set_identity_kernel(cplx* const* __restrict__ As, int n, double 
   }
 }
 
-// C = alpha*A + beta*B + delta*I
+// C = alpha*A + beta*B + delta*I; a null A or B stands for zero
 __global__ void axpby_kernel(const cplx* const* __restrict__ As, const cplx* const* __restrict__ Bs,
                              cplx* const* __restrict__ Cs, cplx alpha, cplx beta, double delta, int n) {
   const cplx* a = As[blockIdx.y];
@@ -136,7 +136,7 @@ __global__ void axpby_kernel(const cplx* const* __restrict__ As, const cplx* con
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
        idx += (long long)gridDim.x * blockDim.x) {
     int j = (int)(idx / n), i = (int)(idx - (long long)j * n);
-    cplx v = cmul(alpha, a[idx]);
+    cplx v = a ? cmul(alpha, a[idx]) : mk(0.0, 0.0);
     if (b) v = cfma(beta, b[idx], v);
     if (i == j) v.x += delta;
     c[idx] = v;
