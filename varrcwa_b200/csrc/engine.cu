@@ -302,9 +302,20 @@ void Engine::free_mat(cplx* p, int n) {
 void Engine::free_vec(cplx* p, int n) {
   if (p) pool((size_t)((n + 15) / 16) * 256).put(p);
 }
-void* Engine::bytes(size_t b) { return pool((b + 255) / 256 * 256).get(); }
+// Size classes of untyped blocks (descriptor arrays, status words, scratch):
+// quarter-octave steps (at most 25% over the request), so that requests
+// whose size follows the batch (every level and wave has its own) share a
+// few pools instead of opening one, with its own chunk, per distinct size.
+static size_t byte_class(size_t b) {
+  b = std::max<size_t>(b, 256);
+  int e = 63 - __builtin_clzll((unsigned long long)b);  // 2^e <= b < 2^(e+1)
+  const size_t unit = (size_t)1 << (e - 2);             // e >= 8
+  size_t c = (b + unit - 1) / unit * unit;
+  return (c + 255) / 256 * 256;
+}
+void* Engine::bytes(size_t b) { return pool(byte_class(b)).get(); }
 void Engine::free_bytes(void* p, size_t b) {
-  if (p) pool((b + 255) / 256 * 256).put(p);
+  if (p) pool(byte_class(b)).put(p);
 }
 
 // Launch arguments (descriptor and pointer arrays) are staged in two halves
