@@ -87,6 +87,14 @@ struct Timed {
       std::sort(g.rbegin(), g.rend());
       fprintf(stderr, "[vrc host] GPU gaps between profiled families: %.1f ms total\n", tot);
       for (size_t q = 0; q < g.size() && q < 12; ++q) fprintf(stderr, "  %8.1f ms  %s\n", g[q].first, g[q].second.c_str());
+      auto rep = [](const char* who, const vrc::Engine& e) {
+        size_t held, out, np, ws;
+        e.pool_report(&held, &out, &np, &ws);
+        fprintf(stderr, "[vrc host] %s: pools %zu, held %.2f GB, handed out %.2f GB, workspace %.2f GB\n", who, np,
+                held / 1e9, out / 1e9, ws / 1e9);
+      };
+      rep("engine", *ctx->eng);
+      for (size_t q = 0; q < ctx->lanes.size(); ++q) rep("lane", *ctx->lanes[q]);
     }
     VRC_CUDA_CHECK(cudaEventRecord(ctx->ev1, ctx->eng->stream()));
     VRC_CUDA_CHECK(cudaEventSynchronize(ctx->ev1));

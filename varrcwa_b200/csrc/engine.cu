@@ -164,6 +164,7 @@ void* BlockPool::get() {
       }
     }
     chunks_.push_back(chunk);
+    blocks_ += per;
     for (size_t i = 0; i < per; ++i) free_.push_back((char*)chunk + i * bytes_);
   }
   void* p = free_.back();
@@ -357,11 +358,21 @@ void* Engine::workspace(size_t nbytes) {
   return ws_;
 }
 
+void Engine::pool_report(size_t* held, size_t* out, size_t* npools, size_t* ws) const {
+  *held = *out = 0;
+  *npools = pools_.size();
+  for (const auto& kv : pools_) {
+    *held += kv.second->blocks() * kv.first;
+    *out += (kv.second->blocks() - kv.second->free_blocks()) * kv.first;
+  }
+  *ws = ws_cap_;
+}
+
 size_t Engine::batch_budget_bytes() const {
   size_t fr = 0, tot = 0;
   cudaMemGetInfo(&fr, &tot);
   size_t b = fr / 4;
-  const size_t cap = (size_t)24 << 30;
+  const size_t cap = (size_t)8 << 30;  // per engine: the lanes each hold one workspace
   if (b > cap) b = cap;
   if (b < ((size_t)256 << 20)) b = (size_t)256 << 20;
   return b;

@@ -110,9 +110,12 @@ class BlockPool {
   void* get();
   void put(void* p) { free_.push_back(p); }
   size_t bytes() const { return bytes_; }
+  size_t blocks() const { return blocks_; }       // blocks created
+  size_t free_blocks() const { return free_.size(); }
 
  private:
   size_t bytes_;
+  size_t blocks_ = 0;
   std::vector<void*> free_;
   std::vector<void*> chunks_;
 };
@@ -143,6 +146,9 @@ class Engine {
     return upload(v.data(), v.size());
   }
   void* workspace(size_t bytes);
+  // diagnostic: bytes held by the pools and the workspace, and the part of
+  // the pools handed out (not returned), summed over the pools
+  void pool_report(size_t* held, size_t* out, size_t* npools, size_t* ws) const;
   size_t batch_budget_bytes() const;
 
   // batched primitives
