@@ -54,7 +54,8 @@ def parse():
                    help="cells per step per GPU (c3: 64 cells per wave; c2 / c4: 128; c1: 8, whose ~6600 "
                         "segments per cell are all held until the star reduction)")
     p.add_argument("--queue", type=int, default=4096, help="c3: cells in the job queue (sharded over ranks)")
-    p.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4"])
+    p.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4", "c5"],
+                   help="c5: config-5 mode converters, forward + adjoint of --batch cells (one GPU)")
     p.add_argument("--pe", type=float, default=None, help="varRCWA tolerance (default 1e-6 for c1, else 1e-2)")
     p.add_argument("--npix", type=int, default=256)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -74,7 +75,7 @@ def parse():
     if a.pe is None:
         a.pe = 1e-6 if a.workload == "c1" else 1e-2
     if a.batch is None:
-        a.batch = {"c1": 8, "c3": 64}.get(a.workload, 128)
+        a.batch = {"c1": 8, "c3": 64, "c5": 4}.get(a.workload, 128)
     return a
 
 
@@ -698,6 +699,24 @@ def measure_c5(ctx, fp64_peak=None, orders=21, batch=2, steps=1, length=20.0, nc
     return line
 
 
+def run_c5(a):
+    """The config-5 forward + adjoint as a line of its own (one GPU): --batch
+    converter cells per step, --steps timed steps, the oracle sample for the
+    CPU baseline unless --no-cpu-baseline."""
+    import torch
+    from varrcwa_b200.capi import Context
+    ctx = Context(0)
+    fp64_peak = dgemm_peak_tflops(0)
+    torch.cuda.empty_cache()
+    clocks = ClockSampler(0)
+    clocks.start()
+    line = measure_c5(ctx, fp64_peak, orders=21, batch=a.batch, steps=a.steps, cpu=not a.no_cpu_baseline)
+    line["clocks"] = clocks.stop()
+    line.update({"n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                 "dtype": "complex128", "data": "synthetic"})
+    print(json.dumps(line), flush=True)
+
+
 def run_kernel(a):
     """One C-ABI kernel entry (vrc_zgemm: batch products of n x n complex
     matrices; vrc_eig: batch eigen-decompositions) on seeded random inputs:
@@ -766,6 +785,9 @@ def main():
         sys.exit(f"bench.py: --gpus {a.gpus} but WORLD_SIZE={world}: launch one process per GPU")
     if a.kernel:
         run_kernel(a)
+        return
+    if a.workload == "c5" and a.impl == "ours":
+        run_c5(a)
         return
     if a.impl == "reference":
         run_reference(a, rank, world)
