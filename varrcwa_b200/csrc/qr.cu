@@ -81,29 +81,33 @@ __device__ __forceinline__ cplx* log_rot(char* logb, int sweep_cap) {
 }
 
 // Eigenvalues of a small upper Hessenberg matrix A (nb x nb, column-major,
-// nb <= NBMAX) by single-shift QR, serial (one thread).  Used only to pick
-// shifts: on failure to converge the remaining diagonal entries are used.
-__device__ void small_eigvals(cplx* A, int nb, cplx* out) {
+// nb <= NBMAX, shared memory) by single-shift QR, used only to pick shifts
+// (on failure to converge the remaining diagonal entries are used).  One
+// warp (all lanes call it): the reflectors are formed redundantly by every
+// lane from the same shared-memory entries (identical results), and lanes own
+// the columns of each row transform and the rows of each column transform.
+__device__ void small_eigvals_warp(cplx* A, int nb, cplx* out, int lane) {
   auto a = [&](int r, int c) -> cplx& { return A[c * nb + r]; };
   int hi = nb - 1, it = 0;
   while (hi >= 0) {
+    __syncwarp();
     if (hi == 0) {
-      out[0] = a(0, 0);
+      if (lane == 0) out[0] = a(0, 0);
       break;
     }
     int lo = hi;
     while (lo > 0 && cabs1(a(lo, lo - 1)) > EIG_ULP * (cabs1(a(lo - 1, lo - 1)) + cabs1(a(lo, lo)))) --lo;
     if (lo == hi) {
-      out[hi] = a(hi, hi);
+      if (lane == 0) out[hi] = a(hi, hi);
       --hi;
       it = 0;
       continue;
     }
     if (++it > 40) {
-      for (int k = 0; k <= hi; ++k) out[k] = a(k, k);
+      if (lane == 0)
+        for (int k = 0; k <= hi; ++k) out[k] = a(k, k);
       break;
     }
-    // Wilkinson shift from the trailing 2x2 block of [lo, hi]
     const cplx p = a(hi - 1, hi - 1), q = a(hi - 1, hi), r = a(hi, hi - 1), d = a(hi, hi);
     const cplx half = cscale(csub(p, d), 0.5);
     const cplx disc = csqrt(cadd(cmul(half, half), cmul(q, r)));
@@ -120,24 +124,28 @@ __device__ void small_eigvals(cplx* A, int nb, cplx* out) {
         y = a(k + 1, k - 1);
       }
       refl2(x, y, &beta, &tau, &v2);
-      if (k > lo) {
+      __syncwarp();  // every lane has read x, y
+      if (k > lo && lane == 0) {
         a(k, k - 1) = beta;
         a(k + 1, k - 1) = mk(0.0, 0.0);
       }
       const cplx tauc = cconj(tau), v2c = cconj(v2);
-      for (int j = k; j <= hi; ++j) {
+      const int j = k + lane;
+      if (j <= hi) {
         cplx u = a(k, j), w = a(k + 1, j);
         cplx s = cmul(tauc, cadd(u, cmul(v2c, w)));
         a(k, j) = csub(u, s);
         a(k + 1, j) = csub(w, cmul(s, v2));
       }
-      const int re = min(k + 2, hi);
-      for (int rr = lo; rr <= re; ++rr) {
+      __syncwarp();
+      const int re = min(k + 2, hi), rr = lo + lane;
+      if (rr <= re) {
         cplx u = a(rr, k), w = a(rr, k + 1);
         cplx s = cmul(tau, cadd(u, cmul(v2, w)));
         a(rr, k) = csub(u, s);
         a(rr, k + 1) = csub(w, cmul(s, v2c));
       }
+      __syncwarp();
     }
   }
 }
@@ -309,19 +317,23 @@ __global__ void __launch_bounds__(QR_THREADS, MINB)
       if (tid == 0) stamp(0);
       if (l >= i) break;  // H[i][i] isolated
       // Number of bulges and their shifts.
-      if (tid == 0) {
+      if (warp == 0) {
         const int w = i - l + 1;
-        int nb = (its == 10 || its == 20) ? 1 : min(NBMAX, max(1, (w - 4) / 6));
+        const int nb = (its == 10 || its == 20) ? 1 : min(NBMAX, max(1, (w - 4) / 6));
         if (nb == 1) {
-          s_shift[0] = single_shift(H, n, l, i, its);
+          if (lane == 0) s_shift[0] = single_shift(H, n, l, i, its);
         } else {
           const int b0 = i - nb + 1;
-          for (int c = 0; c < nb; ++c)
-            for (int r = 0; r < nb; ++r) s_small[c * nb + r] = (r <= c + 1) ? h(b0 + r, b0 + c) : mk(0.0, 0.0);
-          small_eigvals(s_small, nb, s_shift);
+          for (int idx = lane; idx < nb * nb; idx += 32) {
+            const int c = idx / nb, r = idx - c * nb;
+            s_small[c * nb + r] = (r <= c + 1) ? h(b0 + r, b0 + c) : mk(0.0, 0.0);
+          }
+          small_eigvals_warp(s_small, nb, s_shift, lane);
         }
-        s_nb = nb;
-        stamp(1);
+        if (lane == 0) {
+          s_nb = nb;
+          stamp(1);
+        }
       }
       __syncthreads();
       const int nb = s_nb, m = l;
