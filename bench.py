@@ -359,11 +359,18 @@ def _busy(v):
 
 
 def breakdown_of(stats):
+    busy = {k[1:]: round(v["busy_ms"], 3) for k, v in stats.items() if k.startswith("~")}
+    stats = {k: v for k, v in stats.items() if not k.startswith("~")}
     tot = sum(x["ms"] for x in stats.values()) or 1.0
-    return {k: {"ms": round(v["ms"], 3), "busy_ms": round(_busy(v), 3), "share": round(v["ms"] / tot, 4),
-                "launches": v["launches"],
-                "tflops": round(v["flops"] / (_busy(v) * 1e-3) / 1e12, 3) if v["flops"] and v["ms"] else None}
-            for k, v in sorted(stats.items(), key=lambda kv: -kv[1]["ms"])}
+    out = {k: {"ms": round(v["ms"], 3), "busy_ms": round(_busy(v), 3), "share": round(v["ms"] / tot, 4),
+               "launches": v["launches"],
+               "tflops": round(v["flops"] / (_busy(v) * 1e-3) / 1e12, 3) if v["flops"] and v["ms"] else None}
+           for k, v in sorted(stats.items(), key=lambda kv: -kv[1]["ms"])}
+    if "host_alloc" in out:  # host time in cudaMalloc / cudaFree (all engines); its byte slot counts the calls
+        out["host_alloc"]["calls"] = int(stats["host_alloc"]["bytes"])
+    if busy:  # GPU time with at least one kernel of the engines running (all, and per lane)
+        out["gpu_busy_ms"] = busy
+    return out
 
 
 def io_bytes(workload, cells):

@@ -1009,15 +1009,24 @@ int vrc_get_kernel_stats(vrc_context* ctx, int max, vrc_kernel_stat* out) {
     // summed over the lanes: with concurrent lanes a family's time is the
     // sum of its launches' durations, each measured on its own stream
     std::map<std::string, vrc::Engine::FamStat> f = ctx->eng->fam_stats();
-    for (auto& e : ctx->lanes)
-      for (auto& kv : e->fam_stats()) {
+    // "~busy ...": the union of every family's launch intervals, on all
+    // engines and on each one (GPU time with at least one kernel running)
+    auto& all = f["~busy all"];
+    for (auto& kv : f)
+      if (kv.first[0] != '~') all.iv.insert(all.iv.end(), kv.second.iv.begin(), kv.second.iv.end());
+    for (size_t q = 0; q < ctx->lanes.size(); ++q) {
+      auto& mine = f["~busy lane " + std::to_string(q)];
+      for (auto& kv : ctx->lanes[q]->fam_stats()) {
         auto& d = f[kv.first];
         d.ms += kv.second.ms;
         d.launches += kv.second.launches;
         d.flops += kv.second.flops;
         d.bytes += kv.second.bytes;
         d.iv.insert(d.iv.end(), kv.second.iv.begin(), kv.second.iv.end());
+        all.iv.insert(all.iv.end(), kv.second.iv.begin(), kv.second.iv.end());
+        mine.iv.insert(mine.iv.end(), kv.second.iv.begin(), kv.second.iv.end());
       }
+    }
     for (auto& kv : f) {
       if (out && count < max) {
         vrc_kernel_stat& o = out[count];

@@ -138,8 +138,10 @@ BlockPool::~BlockPool() {
 namespace {
 // host time spent in cudaMalloc/cudaFree (all engines), in microseconds
 std::atomic<long long> g_host_alloc_us{0};
+std::atomic<long long> g_host_alloc_calls{0};
 struct AllocTimer {
   std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+  AllocTimer() { ++g_host_alloc_calls; }
   ~AllocTimer() {
     g_host_alloc_us += (long long)std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0)
                            .count();
@@ -147,17 +149,24 @@ struct AllocTimer {
 };
 }  // namespace
 
-void* BlockPool::get() {
+// Chunks come from the device's stream-ordered allocator (cudaMallocAsync on
+// the engine's stream): a plain cudaMalloc while other engines' kernels run
+// took tens of milliseconds per call on B200.  A pool grows by at least a
+// quarter of what it holds (64 MB .. 512 MB per chunk), so a pool that keeps
+// growing over many waves makes few calls.
+void* BlockPool::get(cudaStream_t st) {
   if (free_.empty()) {
     AllocTimer at;
     size_t per = std::max<size_t>(1, (size_t)(64u << 20) / bytes_);
     if (per > 256) per = 256;
+    per = std::max(per, blocks_ / 4);
+    per = std::min(per, std::max<size_t>(1, (size_t)(512u << 20) / bytes_));
     void* chunk = nullptr;
-    cudaError_t e = cudaMalloc(&chunk, per * bytes_);
+    cudaError_t e = cudaMallocAsync(&chunk, per * bytes_, st);
     if (e != cudaSuccess) {
       (void)cudaGetLastError();
       per = 1;
-      e = cudaMalloc(&chunk, bytes_);
+      e = cudaMallocAsync(&chunk, bytes_, st);
       if (e != cudaSuccess) {
         (void)cudaGetLastError();
         throw StatusError(ST_ENOMEM, "device memory exhausted");
@@ -174,6 +183,14 @@ void* BlockPool::get() {
 
 Engine::Engine(int device) : device_(device) {
   VRC_CUDA_CHECK(cudaSetDevice(device));
+  {
+    // the stream-ordered allocator keeps what it has reserved (blocks are
+    // recycled by the pools; freed memory stays reserved for the next chunk)
+    cudaMemPool_t mp;
+    VRC_CUDA_CHECK(cudaDeviceGetDefaultMemPool(&mp, device));
+    uint64_t keep = UINT64_MAX;
+    VRC_CUDA_CHECK(cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &keep));
+  }
   VRC_CUDA_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   own_stream_ = true;
   stage_cap_ = (size_t)128 << 20;  // two halves of 64 MB
@@ -196,6 +213,9 @@ Engine::~Engine() {
   if (d_stage_) cudaFree(d_stage_);
   if (h_stage_) cudaFreeHost(h_stage_);
   if (own_stream_) cudaStreamDestroy(stream_);
+  // hand the stream-ordered allocator's unused reserve back to the device
+  cudaMemPool_t mp;
+  if (cudaDeviceGetDefaultMemPool(&mp, device_) == cudaSuccess) cudaMemPoolTrimTo(mp, 0);
 }
 
 static double host_now_ms() {
@@ -261,12 +281,14 @@ void Engine::set_profiling(bool on) {
 std::map<std::string, Engine::FamStat>& Engine::fam_stats() {
   sync();
   fam_["host_alloc"].ms = 1e-3 * (double)g_host_alloc_us.load() - alloc_ms0_;
+  fam_["host_alloc"].bytes = (double)(g_host_alloc_calls.load() - alloc_calls0_);  // the number of calls
   return fam_;
 }
 void Engine::reset_fam_stats() {
   sync();
   fam_.clear();
   alloc_ms0_ = 1e-3 * (double)g_host_alloc_us.load();
+  alloc_calls0_ = g_host_alloc_calls.load();
 }
 
 Engine::Prof::Prof(Engine& eng, const char* f, double fl, double by, int nlaunch)
@@ -295,8 +317,8 @@ BlockPool& Engine::pool(size_t bytes) {
   return *it->second;
 }
 
-cplx* Engine::mat(int n) { return (cplx*)pool((size_t)n * n * 16).get(); }
-cplx* Engine::vec(int n) { return (cplx*)pool((size_t)((n + 15) / 16) * 256).get(); }
+cplx* Engine::mat(int n) { return (cplx*)pool((size_t)n * n * 16).get(stream_); }
+cplx* Engine::vec(int n) { return (cplx*)pool((size_t)((n + 15) / 16) * 256).get(stream_); }
 void Engine::free_mat(cplx* p, int n) {
   if (p) pool((size_t)n * n * 16).put(p);
 }
@@ -314,7 +336,7 @@ static size_t byte_class(size_t b) {
   size_t c = (b + unit - 1) / unit * unit;
   return (c + 255) / 256 * 256;
 }
-void* Engine::bytes(size_t b) { return pool(byte_class(b)).get(); }
+void* Engine::bytes(size_t b) { return pool(byte_class(b)).get(stream_); }
 void Engine::free_bytes(void* p, size_t b) {
   if (p) pool(byte_class(b)).put(p);
 }
@@ -343,12 +365,12 @@ void* Engine::stage(const void* data, size_t nbytes) {
 
 void* Engine::workspace(size_t nbytes) {
   if (nbytes > ws_cap_) {
-    sync();
+    // stream order: the kernels queued before still use the old workspace
     AllocTimer at;
-    if (ws_) cudaFree(ws_);
+    if (ws_) VRC_CUDA_CHECK(cudaFreeAsync(ws_, stream_));
     ws_ = nullptr;
     size_t cap = nbytes + nbytes / 4;
-    if (cudaMalloc(&ws_, cap) != cudaSuccess) {
+    if (cudaMallocAsync(&ws_, cap, stream_) != cudaSuccess) {
       (void)cudaGetLastError();
       ws_cap_ = 0;
       throw StatusError(ST_ENOMEM, "workspace allocation failed");
@@ -1130,14 +1152,15 @@ void Engine::eig(std::vector<EigReq>& reqs, int n, std::vector<int>* status) {
     }
     if (std::getenv("VRC_QR_STATS")) {
       // diagnostic: per-matrix QR counters from the rotation-log headers
-      double tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      double tot[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
       for (size_t b = 0; b < B; ++b) {
         int hh[4];
-        long long tt[4];
+        long long tt[6];
         VRC_CUDA_CHECK(cudaMemcpyAsync(hh, logs[b], sizeof(hh), cudaMemcpyDeviceToHost, stream_));
         VRC_CUDA_CHECK(cudaMemcpyAsync(tt, (char*)logs[b] + 16, sizeof(tt), cudaMemcpyDeviceToHost, stream_));
         sync();
-        for (int q = 0; q < 4; ++q) tot[q] += hh[q], tot[4 + q] += (double)tt[q];
+        for (int q = 0; q < 4; ++q) tot[q] += hh[q];
+        for (int q = 0; q < 6; ++q) tot[4 + q] += (double)tt[q];
       }
       {
         // sweep-size profile of the first matrix: rounds spent in sweeps on
@@ -1163,10 +1186,11 @@ void Engine::eig(std::vector<EigReq>& reqs, int n, std::vector<int>* status) {
                 cnt[0], cls[0], cnt[1], cls[1], cnt[2], cls[2], cnt[3], cls[3], cnt[4], cls[4], cnt[5], cls[5]);
       }
       fprintf(stderr,
-              "[vrc qr] n=%d matrices=%zu per matrix: sweeps=%.1f rounds=%.0f rotation slots=%.0f (%.2f n^2) "
-              "Mcycles defl=%.2f shift=%.2f rounds=%.2f far=%.2f\n",
-              n, B, tot[0] / B, tot[2] / B, tot[1] / B, tot[1] / B / ((double)n * n), tot[4] / B / 1e6,
-              tot[5] / B / 1e6, tot[6] / B / 1e6, tot[7] / B / 1e6);
+              "[vrc qr] n=%d matrices=%zu per matrix: log entries=%.1f (deflation windows %.1f) rounds=%.0f "
+              "rotation slots=%.0f (%.2f n^2) Mcycles defl=%.2f shift+window=%.2f (window Schur %.2f, "
+              "window deflation %.2f) rounds=%.2f far=%.2f\n",
+              n, B, tot[0] / B, tot[3] / B, tot[2] / B, tot[1] / B, tot[1] / B / ((double)n * n), tot[4] / B / 1e6,
+              tot[5] / B / 1e6, tot[8] / B / 1e6, tot[9] / B / 1e6, tot[6] / B / 1e6, tot[7] / B / 1e6);
     }
     {
       Prof pr(*this, "trevc", (4.0 / 3.0) * nn3 * B, 1.5 * mbytes * B);

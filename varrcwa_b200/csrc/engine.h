@@ -107,7 +107,7 @@ class BlockPool {
  public:
   explicit BlockPool(size_t bytes) : bytes_(bytes) {}
   ~BlockPool();
-  void* get();
+  void* get(cudaStream_t st);  // a new chunk is allocated in stream order on st
   void put(void* p) { free_.push_back(p); }
   size_t bytes() const { return bytes_; }
   size_t blocks() const { return blocks_; }       // blocks created
@@ -383,6 +383,7 @@ class Engine {
   double t_sync_ret_ = -1.0;
  private:
   double alloc_ms0_ = 0.0;
+  long long alloc_calls0_ = 0;
   struct PendingProf {
     const char* fam;
     cudaEvent_t a, b;

@@ -29,7 +29,13 @@
 //
 // Deflation: small subdiagonals (Ahues-Tisseur test) split the window;
 // exceptional shifts at iterations 10 and 20; at most 30*max(10,n)
-// iterations per eigenvalue and 30n+300 in total, else ST_ENOCONV.
+// iterations per eigenvalue and 30n+300 in total, else ST_ENOCONV.  Before
+// a sweep, aggressive early deflation examines the trailing jw x jw block of
+// the window (aed_* below): its converged eigenvalues deflate at once, and
+// its unconverged ones are the sweep's shifts.  Its similarity transform U is
+// applied eagerly inside the active window and logged as a dense block for
+// the replay, in sequence with the sweeps' rotations.
+#include <algorithm>
 #include <cstdlib>
 
 #include "common.cuh"
@@ -50,15 +56,18 @@ constexpr size_t QR_SMEM = (size_t)(QD * QLD + 2 * NBMAX * QB) * sizeof(cplx);
 
 struct QrLogHeader {
   int nsweeps, nrot;
-  int nrounds, pad0;                           // statistics
+  int nrounds, naed;                           // statistics (naed: deflation-window blocks)
   long long t_defl, t_shift, t_rounds, t_far;  // statistics: SM clock cycles per phase
-  long long pad[2];
+  long long t_wschur, t_wdefl;                 // statistics: window Schur form, window deflation
 };
 constexpr int QR_HDR = sizeof(QrLogHeader);  // 64
 // A sweep on the active window [m, i] with nb bulges and R rounds; its
 // rotations are stored round-major from rotation index start: round u,
 // bulge b at start + u*nb + b, acting on the pair (k, k+1), k = m + u - 3b,
-// when m <= k <= i - 1 (other slots are padding and never read).
+// when m <= k <= i - 1 (other slots are padding and never read).  A
+// deflation-window block on the active window [m, i] has nb = -1: the
+// unitary U of order R (columns and rows pad0..i) is stored column-major
+// (leading dimension R) from rotation index start.
 struct QrSweep {
   int m, i, nb, R;
   int start, pad0, pad1, pad2;
@@ -228,12 +237,249 @@ __device__ __forceinline__ void carry_chain(cplx* p0, size_t stride, int cnt, co
   p0[(size_t)cnt * stride] = c;
 }
 
+// ---------------------------------------------------------------------------
+// Aggressive early deflation (Braman, Byers & Mathias, "The multishift QR
+// algorithm. Part II: aggressive early deflation", SIAM J. Matrix Anal.
+// Appl. 23 (2002); LAPACK xLAQR3).  The trailing jw x jw block of the active
+// window (jw <= AW, one lane per row or column) is brought to Schur form
+// T = U^H H_w U by one warp in shared memory.  The subdiagonal entry s0 that
+// couples the block to the rest becomes the spike s0 * conj(U[0, :]); an
+// eigenvalue whose spike entry is negligible deflates, the others are moved
+// to the top of T by swaps of adjacent diagonal entries.  If any deflated,
+// the undeflated top block with its spike is returned to Hessenberg form
+// (one reflector, then a Householder reduction) and U is applied to the rows
+// of the active window above the block; the rest of H and Z receive U through
+// the log (a dense entry, replayed like the sweeps).  The undeflated
+// eigenvalues become the next sweep's shifts.
+constexpr int AW = 32;       // largest deflation window
+constexpr int ALD = AW + 1;  // its leading dimension in shared memory (odd in 16-byte units)
+
+// Givens rotation [cs sn; -conj(sn) cs] (cs real) with cs f + sn g = r and
+// -conj(sn) f + cs g = 0.
+__device__ __forceinline__ void givens(cplx f, cplx g, double* cs, cplx* sn) {
+  const double ag = hypot(g.x, g.y);
+  if (ag == 0.0) {
+    *cs = 1.0;
+    *sn = mk(0.0, 0.0);
+    return;
+  }
+  const double af = hypot(f.x, f.y);
+  if (af == 0.0) {
+    *cs = 0.0;
+    *sn = cscale(cconj(g), 1.0 / ag);
+    return;
+  }
+  const double d = hypot(af, ag);
+  *cs = af / d;
+  *sn = cscale(cmul(cscale(f, 1.0 / af), cconj(g)), 1.0 / d);
+}
+
+// Negligible subdiagonal entry T[k][k-1] of a small window (the test of the
+// main iteration: Ahues-Tisseur, LAPACK xLAHQR).
+__device__ __forceinline__ bool small_negligible(const cplx* T, int nw, int k, double smlnum) {
+  auto t = [&](int r, int c) { return T[c * ALD + r]; };
+  const double cs = cabs1(t(k, k - 1));
+  if (cs <= smlnum) return true;
+  const cplx dkm = t(k - 1, k - 1), dk = t(k, k);
+  double tst = cabs1(dkm) + cabs1(dk);
+  if (tst == 0.0) {
+    if (k - 2 >= 0) tst += fabs(t(k - 1, k - 2).x);
+    if (k + 1 <= nw - 1) tst += fabs(t(k + 1, k).x);
+  }
+  if (cs > EIG_ULP * tst) return false;
+  const double a1 = cs, a2 = cabs1(t(k - 1, k));
+  const double ab = fmax(a1, a2), ba = fmin(a1, a2);
+  const double b1 = cabs1(dk), b2 = cabs1(csub(dkm, dk));
+  const double aa = fmax(b1, b2), bb = fmin(b1, b2);
+  const double s = aa + ab;
+  return ba * (ab / s) <= fmax(smlnum, EIG_ULP * (bb * (aa / s)));
+}
+
+// Schur form of the nw x nw upper Hessenberg T (shared memory, leading
+// dimension ALD) by single-shift QR with Wilkinson shifts (exceptional at
+// iterations 10 and 20), accumulating the rotations into U.  One warp; lanes
+// own the columns of a row transform and the rows of a column transform.
+// Returns false if an eigenvalue needs more than 30 * max(10, nw) iterations.
+__device__ bool small_schur_warp(cplx* T, cplx* U, int nw, int lane, double smlnum) {
+  auto t = [&](int r, int c) -> cplx& { return T[c * ALD + r]; };
+  auto u = [&](int r, int c) -> cplx& { return U[c * ALD + r]; };
+  const int itmax = 30 * max(10, nw);
+  int hi = nw - 1, its = 0;
+  while (hi > 0) {
+    __syncwarp();
+    // largest k <= hi with a negligible T[k][k-1] (lane k-1 tests k), else 0
+    const bool negl = lane + 1 <= hi && small_negligible(T, nw, lane + 1, smlnum);
+    const unsigned bal = __ballot_sync(0xffffffffu, negl);
+    const int lo = bal ? 32 - __clz(bal) : 0;
+    if (lo > 0 && lane == 0) t(lo, lo - 1) = mk(0.0, 0.0);
+    __syncwarp();
+    if (lo == hi) {
+      --hi;
+      its = 0;
+      continue;
+    }
+    if (++its > itmax) return false;
+    const cplx sh = single_shift(T, ALD, lo, hi, its);
+    for (int k = lo; k < hi; ++k) {
+      cplx x, y, beta, tau, v2;
+      __syncwarp();
+      if (k == lo) {
+        x = csub(t(lo, lo), sh);
+        y = t(lo + 1, lo);
+      } else {
+        x = t(k, k - 1);
+        y = t(k + 1, k - 1);
+      }
+      refl2(x, y, &beta, &tau, &v2);
+      __syncwarp();  // every lane has read x, y
+      if (k > lo && lane == 0) {
+        t(k, k - 1) = beta;
+        t(k + 1, k - 1) = mk(0.0, 0.0);
+      }
+      const int j = k + lane;  // row transform over columns k..nw-1 (nw - k <= 32)
+      if (j < nw) rotate2<true>(t(k, j), t(k + 1, j), tau, v2);
+      __syncwarp();
+      if (lane <= min(k + 2, hi)) rotate2<false>(t(lane, k), t(lane, k + 1), tau, v2);
+      if (lane < nw) rotate2<false>(u(lane, k), u(lane, k + 1), tau, v2);
+    }
+  }
+  __syncwarp();
+  return true;
+}
+
+// Swaps the adjacent diagonal entries k, k+1 of the upper triangular T and
+// updates U (LAPACK xTREXC's step: T <- G T G^H, U <- U G^H).  One warp.
+__device__ void schur_swap_warp(cplx* T, cplx* U, int nw, int k, int lane) {
+  auto t = [&](int r, int c) -> cplx& { return T[c * ALD + r]; };
+  auto u = [&](int r, int c) -> cplx& { return U[c * ALD + r]; };
+  const cplx t11 = t(k, k), t22 = t(k + 1, k + 1);
+  double cs;
+  cplx sn;
+  givens(t(k, k + 1), csub(t22, t11), &cs, &sn);
+  const cplx snc = cconj(sn);
+  __syncwarp();
+  const int j = k + 2 + lane;
+  if (j < nw) {  // rows k, k+1 over columns k+2..nw-1
+    const cplx x = t(k, j), y = t(k + 1, j);
+    t(k, j) = cadd(cscale(x, cs), cmul(sn, y));
+    t(k + 1, j) = csub(cscale(y, cs), cmul(snc, x));
+  }
+  if (lane < k) {  // columns k, k+1 over rows 0..k-1
+    const cplx x = t(lane, k), y = t(lane, k + 1);
+    t(lane, k) = cadd(cscale(x, cs), cmul(snc, y));
+    t(lane, k + 1) = csub(cscale(y, cs), cmul(sn, x));
+  }
+  if (lane < nw) {
+    const cplx x = u(lane, k), y = u(lane, k + 1);
+    u(lane, k) = cadd(cscale(x, cs), cmul(snc, y));
+    u(lane, k + 1) = csub(cscale(y, cs), cmul(sn, x));
+  }
+  __syncwarp();
+  if (lane == 0) {
+    t(k, k) = t22;
+    t(k + 1, k + 1) = t11;
+  }
+  __syncwarp();
+}
+
+// Reflector I - tau v v^H (v in shared memory, v[0] = 1) from the left,
+// conjugated, on rows r0..r0+len-1 of T over columns c0..nc-1, and from the
+// right on columns c0'..c0'+len-1 of a matrix over rows 0..nr-1.
+__device__ __forceinline__ void refl_left_warp(cplx* T, const cplx* v, int r0, int len, cplx tau, int c0, int nc,
+                                               int lane) {
+  const int c = c0 + lane;
+  if (c < nc) {
+    cplx w = mk(0.0, 0.0);
+    for (int q = 0; q < len; ++q) w = cadd(w, cmulc(v[q], T[c * ALD + r0 + q]));
+    w = cmul(cconj(tau), w);
+    for (int q = 0; q < len; ++q) T[c * ALD + r0 + q] = csub(T[c * ALD + r0 + q], cmul(v[q], w));
+  }
+}
+__device__ __forceinline__ void refl_right_warp(cplx* M, const cplx* v, int c0, int len, cplx tau, int nr,
+                                                int lane) {
+  if (lane < nr) {
+    cplx w = mk(0.0, 0.0);
+    for (int q = 0; q < len; ++q) w = cadd(w, cmul(M[(c0 + q) * ALD + lane], v[q]));
+    w = cmul(tau, w);
+    for (int q = 0; q < len; ++q) M[(c0 + q) * ALD + lane] = csub(M[(c0 + q) * ALD + lane], cmul(w, cconj(v[q])));
+  }
+}
+
+// Warp sum of a real value.
+__device__ __forceinline__ double warp_sum(double x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  return x;
+}
+
+// The deflation window's analysis by one warp (after small_schur_warp):
+// deflation of the eigenvalues with negligible spike entries, reordering of
+// the others to the top, their values into ev[0..ns-1], and, if anything
+// deflated, the return of the top ns x ns block to Hessenberg form.
+// Returns ns, the number of undeflated eigenvalues.
+__device__ int aed_deflate_warp(cplx* T, cplx* U, cplx* v, cplx* ev, int nw, cplx s0, int lane, double smlnum) {
+  auto t = [&](int r, int c) -> cplx& { return T[c * ALD + r]; };
+  auto u = [&](int r, int c) -> cplx& { return U[c * ALD + r]; };
+  int ns = nw, ilst = 0;
+  const double as0 = cabs1(s0);
+  for (int knt = 0; knt < nw; ++knt) {
+    double foo = cabs1(t(ns - 1, ns - 1));
+    if (foo == 0.0) foo = as0;
+    if (as0 * cabs1(u(0, ns - 1)) <= fmax(smlnum, EIG_ULP * foo)) {
+      --ns;  // converged: stays below the undeflated block
+    } else {
+      for (int k = ns - 2; k >= ilst; --k) schur_swap_warp(T, U, nw, k, lane);  // move it to position ilst
+      ++ilst;
+    }
+  }
+  if (lane < ns) ev[lane] = t(lane, lane);
+  __syncwarp();
+  if (ns == nw || ns <= 1 || (s0.x == 0.0 && s0.y == 0.0)) return ns;
+  // reflector taking the spike's top ns entries to a multiple of e_0
+  {
+    const cplx sp = lane < ns ? cmul(s0, cconj(u(0, lane))) : mk(0.0, 0.0);
+    const double xn2 = warp_sum(lane >= 1 ? cabs2(sp) : 0.0);
+    const cplx alpha = mk(__shfl_sync(0xffffffffu, sp.x, 0), __shfl_sync(0xffffffffu, sp.y, 0));
+    double beta;
+    cplx tau, scale;
+    householder(alpha, xn2, &beta, &tau, &scale);
+    if (lane < ns) v[lane] = lane == 0 ? mk(1.0, 0.0) : cmul(sp, scale);
+    __syncwarp();
+    refl_left_warp(T, v, 0, ns, tau, 0, nw, lane);
+    __syncwarp();
+    refl_right_warp(T, v, 0, ns, tau, ns, lane);
+    refl_right_warp(U, v, 0, ns, tau, nw, lane);
+    __syncwarp();
+  }
+  // Householder reduction of the top ns x ns block to Hessenberg form
+  for (int j = 0; j + 2 < ns; ++j) {
+    const int len = ns - 1 - j;  // rows j+1..ns-1
+    const cplx xr = (lane >= 1 && lane < len) ? t(j + 1 + lane, j) : mk(0.0, 0.0);
+    const double xn2 = warp_sum(cabs2(xr));
+    const cplx alpha = t(j + 1, j);
+    double beta;
+    cplx tau, scale;
+    householder(alpha, xn2, &beta, &tau, &scale);
+    __syncwarp();  // every lane has read column j
+    if (lane < len) v[lane] = lane == 0 ? mk(1.0, 0.0) : cmul(xr, scale);
+    if (lane == 0) t(j + 1, j) = mk(beta, 0.0);
+    if (lane >= 1 && lane < len) t(j + 1 + lane, j) = mk(0.0, 0.0);
+    __syncwarp();
+    refl_left_warp(T, v, j + 1, len, tau, j + 1, nw, lane);
+    __syncwarp();
+    refl_right_warp(T, v, j + 1, len, tau, ns, lane);
+    refl_right_warp(U, v, j + 1, len, tau, nw, lane);
+    __syncwarp();
+  }
+  return ns;
+}
+
 // MINB: resident CTAs per SM the registers are sized for; with three the
 // carry chains prefetch two entries instead of four (no spills either way).
 template <int MINB>
 __global__ void __launch_bounds__(QR_THREADS, MINB)
     hqr_kernel(cplx* const* __restrict__ Hs, void* const* __restrict__ logs, cplx* const* __restrict__ Ws, int n,
-               int sweep_cap, long long rot_cap, int* __restrict__ status) {
+               int sweep_cap, long long rot_cap, int* __restrict__ status, int aed_min, int aed_w) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx* D = reinterpret_cast<cplx*>(smem_raw);  // [QD][QLD] column-major window
   cplx* s_tau = D + QD * QLD;                   // [NBMAX][QB]
@@ -242,7 +488,12 @@ __global__ void __launch_bounds__(QR_THREADS, MINB)
   __shared__ cplx s_small[NBMAX * NBMAX];
   __shared__ int s_red[QR_THREADS / 32];
   __shared__ int s_l, s_nb, s_nsw, s_nrot, s_over, s_nround, s_cur;
-  __shared__ long long s_clk[5];  // statistics: phase timers (defl, shift, rounds, far) and the last stamp
+  // deflation window: reflector vector, undeflated eigenvalues, outcome
+  // (undeflated count, or -1 when skipped), shifts it left for the next sweep
+  __shared__ cplx s_aedv[AW], s_aedev[AW];
+  __shared__ int s_aed_ns, s_pend, s_naed;
+  __shared__ long long s_clk[7];  // statistics: phase timers (defl, shift, rounds, far), the last stamp,
+                                  // window Schur form and window deflation
 
   cplx* H = Hs[blockIdx.x];
   char* logb = static_cast<char*>(logs[blockIdx.x]);
@@ -257,10 +508,12 @@ __global__ void __launch_bounds__(QR_THREADS, MINB)
   auto h = [&](int r, int c) -> cplx& { return H[(size_t)c * n + r]; };
   if (tid == 0) {
     s_nsw = 0;
+    s_pend = 0;
+    s_naed = 0;
     s_nrot = 0;
     s_over = 0;
     s_nround = 0;
-    for (int q = 0; q < 5; ++q) s_clk[q] = 0;
+    for (int q = 0; q < 7; ++q) s_clk[q] = 0;
   }
   __syncthreads();
   // tid 0 only: charge the time since the last stamp to phase q
@@ -316,11 +569,109 @@ __global__ void __launch_bounds__(QR_THREADS, MINB)
       l = s_l;
       if (tid == 0) stamp(0);
       if (l >= i) break;  // H[i][i] isolated
+      // Aggressive early deflation on the trailing block of the window
+      // (skipped at the exceptional-shift iterations and while shifts from
+      // the previous one are pending).
+      const bool exceptional = its == 10 || its == 20;
+      if (aed_min > 0 && !exceptional && s_pend == 0 && i - l + 1 >= aed_min) {
+        const int jw = min(aed_w, i - l + 1), kw = i - jw + 1;
+        const cplx s0 = kw > l ? h(kw, kw - 1) : mk(0.0, 0.0);
+        cplx* T = D;               // [AW][ALD]
+        cplx* U = D + AW * ALD;    // [AW][ALD]
+        for (int idx = tid; idx < jw * jw; idx += QR_THREADS) {
+          const int c = idx / jw, r = idx - c * jw;
+          T[c * ALD + r] = (r <= c + 1) ? h(kw + r, kw + c) : mk(0.0, 0.0);
+          U[c * ALD + r] = mk(r == c ? 1.0 : 0.0, 0.0);
+        }
+        __syncthreads();
+        if (warp == 0) {
+          int ns = -1;
+          const long long c0 = clock64();
+          const bool conv = small_schur_warp(T, U, jw, lane, smlnum);
+          const long long c1 = clock64();
+          if (conv) ns = aed_deflate_warp(T, U, s_aedv, s_aedev, jw, s0, lane, smlnum);
+          if (lane == 0) {
+            s_clk[5] += c1 - c0;
+            s_clk[6] += clock64() - c1;
+            // a deflation is logged as a dense jw x jw block; without room, skip it
+            if (ns >= 0 && ns < jw &&
+                (s_nsw + 1 > sweep_cap || (long long)s_nrot + (jw * jw + 1) / 2 > rot_cap))
+              ns = -1;
+            s_aed_ns = ns;
+          }
+        }
+        __syncthreads();
+        const int ns = s_aed_ns;
+        if (ns >= 0 && ns < jw) {
+          // write the block back, the spike's first entry left of it
+          for (int idx = tid; idx < jw * jw; idx += QR_THREADS) {
+            const int c = idx / jw, r = idx - c * jw;
+            h(kw + r, kw + c) = T[c * ALD + r];
+          }
+          if (tid == 0 && kw > l) h(kw, kw - 1) = ns > 0 ? cmul(s0, cconj(U[0])) : mk(0.0, 0.0);
+          // rows l..kw-1 of the window: H[r, kw:i] <- H[r, kw:i] U (a warp per row)
+          for (int r = l + warp; r < kw; r += QR_THREADS / 32) {
+            const cplx hv = lane < jw ? h(r, kw + lane) : mk(0.0, 0.0);
+            cplx acc = mk(0.0, 0.0);
+            for (int k = 0; k < jw; ++k) {
+              const cplx x = mk(__shfl_sync(0xffffffffu, hv.x, k), __shfl_sync(0xffffffffu, hv.y, k));
+              if (lane < jw) acc = cfma(x, U[lane * ALD + k], acc);
+            }
+            if (lane < jw) h(r, kw + lane) = acc;
+          }
+          // the dense log entry: U column-major (leading dimension jw)
+          const int start = s_nrot;
+          for (int idx = tid; idx < jw * jw; idx += QR_THREADS) {
+            const int c = idx / jw, r = idx - c * jw;
+            rot[2 * (size_t)start + idx] = U[c * ALD + r];
+          }
+          __syncthreads();
+          if (tid == 0) {
+            sweeps[s_nsw] = QrSweep{l, i, -1, jw, start, kw, 0, 0};
+            s_nsw += 1;
+            s_nrot += (jw * jw + 1) / 2;
+            s_naed += 1;
+          }
+        }
+        if (ns >= 0) {
+          // shifts: up to NBMAX undeflated eigenvalues of the block, the
+          // smallest in magnitude (LAPACK xLAQR0's choice); ranks by a warp
+          const int ie = i - (jw - ns);
+          const int want = min(NBMAX, max(1, (ie - l + 1 - 4) / 6));
+          if (warp == 0 && ns >= 1) {
+            const int nsh = min(want, ns);
+            if (lane < ns) {
+              const double me = cabs1(s_aedev[lane]);
+              int rank = 0;
+              for (int q = 0; q < ns; ++q) {
+                const double o = cabs1(s_aedev[q]);
+                rank += (o < me || (o == me && q < lane)) ? 1 : 0;
+              }
+              if (rank < nsh) s_shift[rank] = s_aedev[lane];
+            }
+            if (lane == 0) s_pend = nsh;
+          }
+          __syncthreads();
+          // many deflations: skip the sweep and look again (LAPACK's 14%)
+          if (ns < jw && 100 * (jw - ns) > 14 * jw) {
+            if (tid == 0) s_pend = 0;
+            __syncthreads();
+          }
+          // a deflation: isolate the deflated eigenvalues first (the shifts wait)
+          if (ns < jw) {
+            if (tid == 0) stamp(1);
+            continue;
+          }
+        }
+      }
       // Number of bulges and their shifts.
       if (warp == 0) {
         const int w = i - l + 1;
-        const int nb = (its == 10 || its == 20) ? 1 : min(NBMAX, max(1, (w - 4) / 6));
-        if (nb == 1) {
+        const int pend = exceptional ? 0 : s_pend;  // shifts left by the deflation window
+        const int nb0 = exceptional ? 1 : min(NBMAX, max(1, (w - 4) / 6));
+        const int nb = pend > 0 ? min(nb0, pend) : nb0;
+        if (pend > 0) {
+        } else if (nb == 1) {
           if (lane == 0) s_shift[0] = single_shift(H, n, l, i, its);
         } else {
           const int b0 = i - nb + 1;
@@ -330,8 +681,10 @@ __global__ void __launch_bounds__(QR_THREADS, MINB)
           }
           small_eigvals_warp(s_small, nb, s_shift, lane);
         }
+        __syncwarp();  // every lane has read s_pend
         if (lane == 0) {
           s_nb = nb;
+          s_pend = 0;
           stamp(1);
         }
       }
@@ -489,10 +842,13 @@ __global__ void __launch_bounds__(QR_THREADS, MINB)
     hdr->nsweeps = s_nsw;
     hdr->nrot = s_nrot;
     hdr->nrounds = s_nround;
+    hdr->naed = s_naed;
     hdr->t_defl = s_clk[0];
     hdr->t_shift = s_clk[1];
     hdr->t_rounds = s_clk[2];
     hdr->t_far = s_clk[3];
+    hdr->t_wschur = s_clk[5];
+    hdr->t_wdefl = s_clk[6];
     if (failed && status) status[blockIdx.x] = ST_ENOCONV;
   }
 }
@@ -598,8 +954,28 @@ struct ReplayRing {
 };
 
 constexpr int RS = 4 * ReplayRing<RP_NBG, RP_PFD, false>::P;  // rounds per slab (a multiple of the ring size)
-constexpr size_t RP_SMEM =
-    (size_t)RS * NBMAX * 2 * sizeof(cplx) + (size_t)(RP_PFD + 1) * RP_THREADS * sizeof(cplx);
+// staged rotations of a slab, or one deflation-window block (AW x AW)
+constexpr int RP_ROT = RS * NBMAX * 2 > AW * AW ? RS * NBMAX * 2 : AW * AW;
+constexpr size_t RP_SMEM = (size_t)RP_ROT * sizeof(cplx) + (size_t)(RP_PFD + 1) * RP_THREADS * sizeof(cplx);
+
+// A deflation-window block on one vector: x[kw..kw+jw-1] <- U^H x (row
+// transforms, ROWOP) or x U (column transforms); U in shared memory, AW x AW
+// column-major, zero outside jw x jw.
+template <bool ROWOP>
+__device__ __noinline__ void replay_block(cplx* x, size_t stride, int kw, int jw, const cplx* U) {
+  cplx v[AW];
+#pragma unroll
+  for (int k = 0; k < AW; ++k) v[k] = k < jw ? x[(size_t)(kw + k) * stride] : mk(0.0, 0.0);
+  for (int j = 0; j < jw; ++j) {
+    cplx acc = mk(0.0, 0.0);
+#pragma unroll
+    for (int k = 0; k < AW; ++k) {
+      const cplx u = U[j * AW + k];
+      acc = ROWOP ? cadd(acc, cmulc(u, v[k])) : cfma(v[k], u, acc);
+    }
+    x[(size_t)(kw + j) * stride] = acc;
+  }
+}
 
 template <bool ROWOP>
 __device__ __forceinline__ void replay_sweeps(cplx* x, size_t stride, int sel, int idx, const QrSweep* sw,
@@ -614,6 +990,17 @@ __device__ __forceinline__ void replay_sweeps(cplx* x, size_t stride, int sel, i
     const int nb = q.nb;
     const bool active = idx >= 0 && (sel == 0 || (sel == 1 && idx < q.m) || (sel == 2 && idx > q.i));
     const cplx* src = rot + 2 * (size_t)q.start;
+    if (nb < 0) {  // deflation-window block
+      const int jw = q.R;
+      __syncthreads();  // the previous slab is consumed
+      for (int e = threadIdx.x; e < AW * AW; e += blockDim.x) {
+        const int c = e / AW, r = e - c * AW;
+        s_rot[e] = (r < jw && c < jw) ? ld(src + (size_t)c * jw + r) : mk(0.0, 0.0);
+      }
+      __syncthreads();
+      if (active) replay_block<ROWOP>(x, stride, q.pad0, jw, s_rot);
+      continue;
+    }
     for (int b0 = 0; b0 < nb; b0 += RP_NBG) {
       const int ng = min(RP_NBG, nb - b0);
       ReplayRing<RP_NBG, RP_PFD, ROWOP> ring;
@@ -640,7 +1027,7 @@ __global__ void __launch_bounds__(RP_THREADS, 4)
                           void* const* __restrict__ logs, int n, int sweep_cap, int row_blocks) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx* s_rot = reinterpret_cast<cplx*>(smem_raw);
-  cplx* s_pf = s_rot + RS * NBMAX * 2;
+  cplx* s_pf = s_rot + RP_ROT;
   const int mat = blockIdx.y;
   const bool isZ = blockIdx.x >= row_blocks;
   const int r = (isZ ? blockIdx.x - row_blocks : blockIdx.x) * blockDim.x + threadIdx.x;
@@ -657,7 +1044,7 @@ __global__ void __launch_bounds__(RP_THREADS, 4)
     qr_replay_cols_kernel(cplx* const* __restrict__ Hs, void* const* __restrict__ logs, int n, int sweep_cap) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx* s_rot = reinterpret_cast<cplx*>(smem_raw);
-  cplx* s_pf = s_rot + RS * NBMAX * 2;
+  cplx* s_pf = s_rot + RP_ROT;
   const int mat = blockIdx.y;
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   cplx* H = Hs[mat];
@@ -679,6 +1066,21 @@ void schur_batched(cplx* const* d_H, cplx* const* d_Z, cplx* const* d_W, void* c
     return (e && std::atoi(e) == 3) ? 3 : 2;
   }();
   auto hqr = minb == 3 ? hqr_kernel<3> : hqr_kernel<2>;
+  // order of the deflation window (VRC_QR_AEDW, 4..32): measured on B200,
+  // 8 for n <= 128 and 12 above balance the window's cost (one warp) against
+  // the sweeps it saves
+  static const int aed_w_env = [] {
+    const char* e = std::getenv("VRC_QR_AEDW");
+    return e ? std::min(AW, std::max(4, std::atoi(e))) : 0;
+  }();
+  const int aed_w = aed_w_env ? aed_w_env : (n <= 128 ? 8 : 12);
+  // aggressive early deflation on active windows of at least this order
+  // (VRC_QR_AED; default the window's order, 0 turns it off)
+  static const int aed_env = [] {
+    const char* e = std::getenv("VRC_QR_AED");
+    return e ? std::max(0, std::atoi(e)) : -1;
+  }();
+  const int aed_min = aed_env >= 0 ? aed_env : aed_w;
   ensure_smem((const void*)hqr, QR_SMEM);
   ensure_smem((const void*)qr_replay_rows_kernel, RP_SMEM);
   ensure_smem((const void*)qr_replay_cols_kernel, RP_SMEM);
@@ -690,7 +1092,7 @@ void schur_batched(cplx* const* d_H, cplx* const* d_Z, cplx* const* d_W, void* c
     const int nb = min(65535, batch - b0);
     if (parts & SCHUR_ITERATE)
       hqr<<<nb, QR_THREADS, QR_SMEM, st>>>(d_H + b0, d_logs + b0, d_W + b0, n, cc, rc,
-                                                  d_status ? d_status + b0 : nullptr);
+                                                  d_status ? d_status + b0 : nullptr, aed_min, aed_w);
     if (parts & SCHUR_REPLAY) {
       qr_replay_rows_kernel<<<dim3(2 * row_blocks, nb), RP_THREADS, rp_smem, st>>>(d_H + b0, d_Z + b0, d_logs + b0,
                                                                                   n, cc, row_blocks);
