@@ -237,6 +237,103 @@ __device__ __forceinline__ void carry_chain(cplx* p0, size_t stride, int cnt, co
   p0[(size_t)cnt * stride] = c;
 }
 
+// cp.async copies of 16 bytes into shared memory, one commit group each.
+__device__ __forceinline__ void cpa16(cplx* smem, const cplx* g) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpa_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// A group of NBG bulges' rotations applied round by round to one vector x
+// (entries x[c * stride]): in round t bulge g acts on the pair
+// (kb + t - 3g, kb + t - 3g + 1).  Entries arrive PFD rounds ahead through
+// 16-byte cp.async copies into this thread's shared-memory slots (THREADS
+// apart), then move into a ring of registers indexed by compile-time slots
+// (round loops are unrolled by the ring size): each round takes in the entry
+// the leading bulge reaches and retires the one the trailing bulge has
+// passed; the group's rotations within a round touch disjoint pairs and run
+// independently.  Entries outside [lo, hi] are neither read nor written.
+template <int NBG, int PFD, bool ROWOP, int THREADS>
+struct RotRing {
+  static constexpr int L = 3 * (NBG - 1);  // retire lag
+  static constexpr int P = L + 3;          // register ring: entries t-L .. t+1
+  static constexpr int S = PFD + 1;        // shared-memory slots per thread
+  cplx w[P];
+  cplx* x;
+  cplx* pf;  // this thread's slot 0; slot q at pf[q * THREADS]
+  size_t stride;
+  int kb, lo, hi, rmin, cnt;
+
+  __device__ __forceinline__ void begin(cplx* x_, size_t stride_, int kb_, int lo_, int hi_, int ng, int cnt_,
+                                        cplx* pf_) {
+    x = x_;
+    pf = pf_;
+    stride = stride_;
+    kb = kb_;
+    lo = lo_;
+    hi = hi_;
+    rmin = -3 * (ng - 1);
+    cnt = cnt_;
+    if (cnt <= 0) return;
+#pragma unroll
+    for (int q = -L; q <= 0; ++q) {
+      const int c = kb + q;
+      w[(q + P) % P] = (q >= rmin && c >= lo && c <= hi) ? x[(size_t)c * stride] : mk(0.0, 0.0);
+    }
+#pragma unroll
+    for (int d = 1; d <= PFD; ++d) {  // one commit group per entry
+      const int c = kb + d;
+      if (c >= lo && c <= hi) cpa16(pf + (d % S) * THREADS, x + (size_t)c * stride);
+      cpa_commit();
+    }
+  }
+
+  // Rounds [t0, t1) (t0 a multiple of P); rot(t, g, tau, v2) gives bulge g's
+  // rotation of round t, the identity where it is outside the window
+  template <class ROT>
+  __device__ __forceinline__ void run(int t0, int t1, ROT rot) {
+    t1 = min(t1, cnt);
+    for (int tb = t0; tb < t1; tb += P) {
+#pragma unroll
+      for (int tt = 0; tt < P; ++tt) {
+        const int t = tb + tt;
+        if (t < t1) {
+          const int cb = kb + t;
+          cpa_wait<PFD - 1>();  // the group of entry t+1 has landed
+          w[(tt + 1) % P] = (cb + 1 >= lo && cb + 1 <= hi) ? pf[((t + 1) % S) * THREADS] : mk(0.0, 0.0);
+          {
+            const int c = cb + 1 + PFD;  // into the slot of entry t, consumed last round
+            if (c >= lo && c <= hi) cpa16(pf + ((t + 1 + PFD) % S) * THREADS, x + (size_t)c * stride);
+            cpa_commit();
+          }
+#pragma unroll
+          for (int g = 0; g < NBG; ++g) {  // straight-line: inactive pairs carry the identity
+            cplx tau, v2;
+            rot(t, g, tau, v2);
+            rotate2<ROWOP>(w[(tt - 3 * g + 2 * P) % P], w[(tt - 3 * g + 1 + 2 * P) % P], tau, v2);
+          }
+          {
+            const int q = t - L, c = cb - L;
+            if (q >= rmin && c >= lo && c <= hi) x[(size_t)c * stride] = w[(tt - L + 2 * P) % P];
+          }
+          if (t == cnt - 1) {
+#pragma unroll
+            for (int d = 1; d <= L + 1; ++d) {  // entries t-L+1 .. t+1 still held
+              const int q = t - L + d, c = cb - L + d;
+              if (q >= rmin && c >= lo && c <= hi) x[(size_t)c * stride] = w[(tt - L + d + 2 * P) % P];
+            }
+            cpa_wait<0>();  // no copy may land in the slots after this vector is done
+          }
+        }
+      }
+    }
+  }
+};
+
 // ---------------------------------------------------------------------------
 // Aggressive early deflation (Braman, Byers & Mathias, "The multishift QR
 // algorithm. Part II: aggressive early deflation", SIAM J. Matrix Anal.
@@ -720,6 +817,10 @@ __global__ void __launch_bounds__(QR_THREADS, MINB)
         auto dd = [&](int r, int c) -> cplx& { return D[(c - ds) * QLD + (r - ds)]; };
         auto reflect = [&](int r) {
           const int k = m + r - 3 * a;
+          if (lane == 0 && mine && !(k >= m && k <= i - 1)) {  // outside the window: the identity
+            s_tau[a * QB + (r - r0)] = mk(0.0, 0.0);
+            s_v2[a * QB + (r - r0)] = mk(0.0, 0.0);
+          }
           if (lane == 0 && mine && k >= m && k <= i - 1) {
             cplx x, y, beta, tau, v2;
             if (k == m) {
@@ -869,91 +970,7 @@ constexpr int RP_THREADS = 128;
 constexpr int RP_NBG = 4;  // bulges per register ring
 constexpr int RP_PFD = 7;  // prefetch depth in rounds (ring of PFD + 1 = 8 slots)
 
-__device__ __forceinline__ void cpa16(cplx* smem, const cplx* g) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(g) : "memory");
-}
-__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cpa_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
-template <int NBG, int PFD, bool ROWOP>
-struct ReplayRing {
-  static constexpr int L = 3 * (NBG - 1);  // retire lag
-  static constexpr int P = L + 3;          // register ring: entries t-L .. t+1
-  static constexpr int S = PFD + 1;        // shared-memory slots per thread
-  cplx w[P];
-  cplx* x;
-  cplx* pf;  // this thread's slot 0; slot q at pf[q * RP_THREADS]
-  size_t stride;
-  int kb, lo, hi, rmin, cnt;
-
-  __device__ __forceinline__ void begin(cplx* x_, size_t stride_, int kb_, int lo_, int hi_, int ng, int cnt_,
-                                        cplx* pf_) {
-    x = x_;
-    pf = pf_;
-    stride = stride_;
-    kb = kb_;
-    lo = lo_;
-    hi = hi_;
-    rmin = -3 * (ng - 1);
-    cnt = cnt_;
-    if (cnt <= 0) return;
-#pragma unroll
-    for (int q = -L; q <= 0; ++q) {
-      const int c = kb + q;
-      w[(q + P) % P] = (q >= rmin && c >= lo && c <= hi) ? x[(size_t)c * stride] : mk(0.0, 0.0);
-    }
-#pragma unroll
-    for (int d = 1; d <= PFD; ++d) {  // one commit group per entry
-      const int c = kb + d;
-      if (c >= lo && c <= hi) cpa16(pf + (d % S) * RP_THREADS, x + (size_t)c * stride);
-      cpa_commit();
-    }
-  }
-
-  // srot: this group's rotations of rounds [t0, t1), NBG (tau, v2) pairs per
-  // round, identity where a bulge is outside the window or beyond the group
-  __device__ __forceinline__ void run(int t0, int t1, const cplx* __restrict__ srot) {
-    t1 = min(t1, cnt);
-    for (int tb = t0; tb < t1; tb += P) {
-#pragma unroll
-      for (int tt = 0; tt < P; ++tt) {
-        const int t = tb + tt;
-        if (t < t1) {
-          const int cb = kb + t;
-          cpa_wait<PFD - 1>();  // the group of entry t+1 has landed
-          w[(tt + 1) % P] = (cb + 1 >= lo && cb + 1 <= hi) ? pf[((t + 1) % S) * RP_THREADS] : mk(0.0, 0.0);
-          {
-            const int c = cb + 1 + PFD;  // into the slot of entry t, consumed last round
-            if (c >= lo && c <= hi) cpa16(pf + ((t + 1 + PFD) % S) * RP_THREADS, x + (size_t)c * stride);
-            cpa_commit();
-          }
-          const cplx* rr = srot + 2 * NBG * (t - t0);
-#pragma unroll
-          for (int g = 0; g < NBG; ++g)  // straight-line: inactive pairs carry the identity
-            rotate2<ROWOP>(w[(tt - 3 * g + 2 * P) % P], w[(tt - 3 * g + 1 + 2 * P) % P], rr[2 * g], rr[2 * g + 1]);
-          {
-            const int q = t - L, c = cb - L;
-            if (q >= rmin && c >= lo && c <= hi) x[(size_t)c * stride] = w[(tt - L + 2 * P) % P];
-          }
-          if (t == cnt - 1) {
-#pragma unroll
-            for (int d = 1; d <= L + 1; ++d) {  // entries t-L+1 .. t+1 still held
-              const int q = t - L + d, c = cb - L + d;
-              if (q >= rmin && c >= lo && c <= hi) x[(size_t)c * stride] = w[(tt - L + d + 2 * P) % P];
-            }
-            cpa_wait<0>();  // no copy may land in the slots after this vector is done
-          }
-        }
-      }
-    }
-  }
-};
-
-constexpr int RS = 4 * ReplayRing<RP_NBG, RP_PFD, false>::P;  // rounds per slab (a multiple of the ring size)
+constexpr int RS = 4 * RotRing<RP_NBG, RP_PFD, false, RP_THREADS>::P;  // rounds per slab (a multiple of the ring size)
 // staged rotations of a slab, or one deflation-window block (AW x AW)
 constexpr int RP_ROT = RS * NBMAX * 2 > AW * AW ? RS * NBMAX * 2 : AW * AW;
 constexpr size_t RP_SMEM = (size_t)RP_ROT * sizeof(cplx) + (size_t)(RP_PFD + 1) * RP_THREADS * sizeof(cplx);
@@ -1003,7 +1020,7 @@ __device__ __forceinline__ void replay_sweeps(cplx* x, size_t stride, int sel, i
     }
     for (int b0 = 0; b0 < nb; b0 += RP_NBG) {
       const int ng = min(RP_NBG, nb - b0);
-      ReplayRing<RP_NBG, RP_PFD, ROWOP> ring;
+      RotRing<RP_NBG, RP_PFD, ROWOP, RP_THREADS> ring;
       if (active) ring.begin(x, stride, q.m - 3 * b0, q.m, q.i, ng, q.R, s_pf + threadIdx.x);
       for (int t0 = 0; t0 < q.R; t0 += RS) {
         const int nr = min(RS, q.R - t0);
@@ -1016,7 +1033,12 @@ __device__ __forceinline__ void replay_sweeps(cplx* x, size_t stride, int sel, i
           s_rot[2 * e + 1] = on ? ld(q2 + 1) : mk(0.0, 0.0);
         }
         __syncthreads();
-        if (active) ring.run(t0, t0 + nr, s_rot);
+        if (active)
+          ring.run(t0, t0 + nr, [&](int t, int g, cplx& tau, cplx& v2) {
+            const cplx* rr = s_rot + 2 * RP_NBG * (t - t0);
+            tau = rr[2 * g];
+            v2 = rr[2 * g + 1];
+          });
       }
     }
   }
@@ -1067,20 +1089,20 @@ void schur_batched(cplx* const* d_H, cplx* const* d_Z, cplx* const* d_W, void* c
   }();
   auto hqr = minb == 3 ? hqr_kernel<3> : hqr_kernel<2>;
   // order of the deflation window (VRC_QR_AEDW, 4..32): measured on B200,
-  // 8 for n <= 128 and 12 above balance the window's cost (one warp) against
-  // the sweeps it saves
+  // 12 balances the window's cost (one warp) against the sweeps it saves
   static const int aed_w_env = [] {
     const char* e = std::getenv("VRC_QR_AEDW");
     return e ? std::min(AW, std::max(4, std::atoi(e))) : 0;
   }();
-  const int aed_w = aed_w_env ? aed_w_env : (n <= 128 ? 8 : 12);
+  const int aed_w = aed_w_env ? aed_w_env : 12;
   // aggressive early deflation on active windows of at least this order
-  // (VRC_QR_AED; default the window's order, 0 turns it off)
+  // (VRC_QR_AED; 0 turns it off; by default the window's order for n > 128,
+  // off below, where the sweeps it saves cost less than the windows)
   static const int aed_env = [] {
     const char* e = std::getenv("VRC_QR_AED");
     return e ? std::max(0, std::atoi(e)) : -1;
   }();
-  const int aed_min = aed_env >= 0 ? aed_env : aed_w;
+  const int aed_min = aed_env >= 0 ? aed_env : (n <= 128 ? 0 : aed_w);
   ensure_smem((const void*)hqr, QR_SMEM);
   ensure_smem((const void*)qr_replay_rows_kernel, RP_SMEM);
   ensure_smem((const void*)qr_replay_cols_kernel, RP_SMEM);
