@@ -43,6 +43,91 @@ __global__ void pillar_raster_kernel(const double* __restrict__ radius, cplx* co
 }
 
 // ---------------------------------------------------------------------------
+// Grid geometry on the device (the coordinate rules of
+// VarLayerSampler::addXRule / addYRule, src/core/VarLayerSampler.cpp:42-69,
+// tabulated once per structure): per sample the moving coordinates at z, the
+// sorted copy of x and, where coordinates cross, the painter's-order refill
+// of the permittivity columns (src/rcwa/FourierSolver1D.cpp:145-193).
+// ---------------------------------------------------------------------------
+// Rule value at z through knots zs with values vals: linear, or the natural
+// cubic spline with second derivatives M (h = z_hi - z_lo, b = (z - z_lo) / h,
+// a = 1 - b: a y_lo + b y_hi + ((a^3 - a) M_lo + (b^3 - b) M_hi) h^2 / 6);
+// constant beyond the end knots.
+__device__ double rule_eval(double z, const double* zs, const double* vals, const double* M, int K, int spline) {
+  if (K <= 0) return 0.0;
+  if (z <= zs[0]) return vals[0];
+  if (z >= zs[K - 1]) return vals[K - 1];
+  int lo = 0, hi = K - 1;  // zs[lo] <= z < zs[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) / 2;
+    if (zs[mid] <= z) lo = mid;
+    else hi = mid;
+  }
+  const double h = zs[hi] - zs[lo];
+  const double b = (z - zs[lo]) / h, a = 1.0 - b;
+  double x = a * vals[lo] + b * vals[hi];
+  if (spline) x += ((a * a * a - a) * M[lo] + (b * b * b - b) * M[hi]) * h * h / 6.0;
+  return x;
+}
+
+// One block per sample.  Table layout (GridGeomJob): gd = base x (ncx), base
+// y (ncy), then each rule's knots, values and second derivatives at its
+// offset; gi = per rule (axis, index, K, offset, spline).  Rules apply in
+// order (a later rule on the same coordinate wins).  Output: coords = x
+// (ncx), sorted x (ncx), y (ncy); eps_out[slot] = the structure's eps, or
+// the refilled copy in refill where coordinates cross.
+__global__ void grid_geometry_kernel(const GridGeomJob* __restrict__ jobs, int ncx, int ncy, int nr, int nc,
+                                     const cplx** __restrict__ eps_out) {
+  extern __shared__ __align__(16) unsigned char gsm[];
+  double* x = reinterpret_cast<double*>(gsm);
+  int* rindex = reinterpret_cast<int*>(x + ncx);
+  const GridGeomJob jb = jobs[blockIdx.x];
+  const int t = threadIdx.x;
+  double* xo = jb.coords;
+  double* xso = xo + ncx;
+  double* yo = xso + ncx;
+  for (int q = t; q < ncx; q += blockDim.x) x[q] = jb.gd[q];
+  for (int q = t; q < ncy; q += blockDim.x) yo[q] = jb.gd[ncx + q];
+  __syncthreads();
+  if (t == 0) {
+    for (int r = 0; r < jb.nrules; ++r) {
+      const int* g = jb.gi + 5 * r;
+      const double* base = jb.gd + ncx + ncy + g[3];
+      const double v = rule_eval(jb.z, base, base + g[2], base + 2 * g[2], g[2], g[4]);
+      if (g[0] == 0) x[g[1]] = v;
+      else yo[g[1]] = v;
+    }
+  }
+  __syncthreads();
+  // stable rank of each x (ties keep their order): the sorted copy and the
+  // painter's order of the cells
+  int moved = 0;
+  for (int q = t; q < ncx; q += blockDim.x) {
+    const double v = x[q];
+    int rank = 0;
+    for (int j = 0; j < ncx; ++j) rank += (x[j] < v || (x[j] == v && j < q)) ? 1 : 0;
+    rindex[q] = rank;
+    xo[q] = v;
+    xso[rank] = v;
+    moved |= rank != q;
+  }
+  const int need = __syncthreads_or(moved);
+  if (!need) {
+    if (t == 0) eps_out[jb.slot] = jb.eps;
+    return;
+  }
+  // a later cell overrides an earlier one on the columns its sorted span covers
+  for (int e = t; e < nr * nc; e += blockDim.x) {
+    const int row = e / nc, j = e - row * nc;
+    cplx v = jb.eps[e];
+    for (int i = 0; i < nc; ++i)
+      if (x[i] < x[i + 1] && rindex[i] <= j && rindex[i + 1] >= j + 1) v = jb.eps[(size_t)row * nc + i];
+    jb.refill[e] = v;
+  }
+  if (t == 0) eps_out[jb.slot] = jb.refill;
+}
+
+// ---------------------------------------------------------------------------
 // Twiddle tables: T[p][c] column-major (P x ncell), P = 2*nh-1.
 // ---------------------------------------------------------------------------
 __global__ void twiddle_kernel(const double* const* __restrict__ coords, cplx* const* __restrict__ out,
@@ -312,6 +397,14 @@ void pillar_raster(const double* d_radius, cplx* const* d_eps, int batch, int np
   if (batch <= 0) return;
   pillar_raster_kernel<<<grid_for(npx * npy, batch), 256, 0, st>>>(d_radius, d_eps, npx, npy, Lx, Ly, eps_in,
                                                                   eps_out);
+  VRC_CUDA_CHECK(cudaGetLastError());
+}
+
+void grid_geometry(const GridGeomJob* d_jobs, int njobs, int ncx, int ncy, const cplx** d_eps_out, cudaStream_t st) {
+  if (njobs <= 0) return;
+  const size_t sm = (size_t)ncx * (sizeof(double) + sizeof(int));
+  ensure_smem((const void*)grid_geometry_kernel, sm);
+  grid_geometry_kernel<<<njobs, 128, sm, st>>>(d_jobs, ncx, ncy, ncy - 1, ncx - 1, d_eps_out);
   VRC_CUDA_CHECK(cudaGetLastError());
 }
 

@@ -147,6 +147,8 @@ vrc::CellSpec to_spec(const vrc_cell& c) {
         const vrc_rule& r = rs[i];
         if (r.nknots < 1 || !r.zs || !r.vals || r.interp < 0 || r.interp > 1)
           throw vrc::StatusError(VRC_EINVAL, "invalid coordinate rule");
+        if (r.index < 0 || r.index >= (axis == 0 ? c.ncx : c.ncy))
+          throw vrc::StatusError(VRC_EINVAL, "coordinate rule index out of range");
         for (int k = 0; k + 1 < r.nknots; ++k)
           if (!(r.zs[k + 1] > r.zs[k])) throw vrc::StatusError(VRC_EINVAL, "rule knots must increase");
         vrc::PwlRule pr;

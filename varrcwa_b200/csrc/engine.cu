@@ -132,7 +132,41 @@ double CellSpec::radius(double z) const {
 // Memory
 // ---------------------------------------------------------------------------
 BlockPool::~BlockPool() {
-  for (void* c : chunks_) cudaFree(c);
+  for (auto& c : chunks_) cudaFree(c.first);
+}
+
+size_t BlockPool::release_free(cudaStream_t st) {
+  if (free_.empty()) return 0;
+  std::vector<void*> fr(free_);
+  std::sort(fr.begin(), fr.end());
+  std::vector<std::pair<void*, size_t>> keep;
+  size_t released = 0;
+  for (auto& c : chunks_) {
+    char* lo = (char*)c.first;
+    char* hi = lo + c.second * bytes_;
+    const size_t nfree = std::lower_bound(fr.begin(), fr.end(), (void*)hi) - std::lower_bound(fr.begin(), fr.end(), (void*)lo);
+    if (nfree == c.second && cudaFree(c.first) == cudaSuccess) {
+      released += c.second * bytes_;
+      blocks_ -= c.second;
+    } else {
+      keep.push_back(c);
+    }
+  }
+  if (released) {
+    std::vector<void*> nf;
+    for (void* p : free_) {
+      bool kept = false;
+      for (auto& c : keep)
+        if ((char*)p >= (char*)c.first && (char*)p < (char*)c.first + c.second * bytes_) {
+          kept = true;
+          break;
+        }
+      if (kept) nf.push_back(p);
+    }
+    free_.swap(nf);
+    chunks_.swap(keep);
+  }
+  return released;
 }
 
 namespace {
@@ -149,30 +183,23 @@ struct AllocTimer {
 };
 }  // namespace
 
-// Chunks come from the device's stream-ordered allocator (cudaMallocAsync on
-// the engine's stream): a plain cudaMalloc while other engines' kernels run
-// took tens of milliseconds per call on B200.  A pool grows by at least a
-// quarter of what it holds (64 MB .. 512 MB per chunk), so a pool that keeps
-// growing over many waves makes few calls.
-void* BlockPool::get(cudaStream_t st) {
+void* BlockPool::get(cudaStream_t) {
   if (free_.empty()) {
     AllocTimer at;
     size_t per = std::max<size_t>(1, (size_t)(64u << 20) / bytes_);
     if (per > 256) per = 256;
-    per = std::max(per, blocks_ / 4);
-    per = std::min(per, std::max<size_t>(1, (size_t)(512u << 20) / bytes_));
     void* chunk = nullptr;
-    cudaError_t e = cudaMallocAsync(&chunk, per * bytes_, st);
+    cudaError_t e = cudaMalloc(&chunk, per * bytes_);
     if (e != cudaSuccess) {
       (void)cudaGetLastError();
       per = 1;
-      e = cudaMallocAsync(&chunk, bytes_, st);
+      e = cudaMalloc(&chunk, bytes_);
       if (e != cudaSuccess) {
         (void)cudaGetLastError();
-        throw StatusError(ST_ENOMEM, "device memory exhausted");
+        return nullptr;
       }
     }
-    chunks_.push_back(chunk);
+    chunks_.push_back({chunk, per});
     blocks_ += per;
     for (size_t i = 0; i < per; ++i) free_.push_back((char*)chunk + i * bytes_);
   }
@@ -183,14 +210,6 @@ void* BlockPool::get(cudaStream_t st) {
 
 Engine::Engine(int device) : device_(device) {
   VRC_CUDA_CHECK(cudaSetDevice(device));
-  {
-    // the stream-ordered allocator keeps what it has reserved (blocks are
-    // recycled by the pools; freed memory stays reserved for the next chunk)
-    cudaMemPool_t mp;
-    VRC_CUDA_CHECK(cudaDeviceGetDefaultMemPool(&mp, device));
-    uint64_t keep = UINT64_MAX;
-    VRC_CUDA_CHECK(cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &keep));
-  }
   VRC_CUDA_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   own_stream_ = true;
   stage_cap_ = (size_t)128 << 20;  // two halves of 64 MB
@@ -213,9 +232,6 @@ Engine::~Engine() {
   if (d_stage_) cudaFree(d_stage_);
   if (h_stage_) cudaFreeHost(h_stage_);
   if (own_stream_) cudaStreamDestroy(stream_);
-  // hand the stream-ordered allocator's unused reserve back to the device
-  cudaMemPool_t mp;
-  if (cudaDeviceGetDefaultMemPool(&mp, device_) == cudaSuccess) cudaMemPoolTrimTo(mp, 0);
 }
 
 static double host_now_ms() {
@@ -317,8 +333,25 @@ BlockPool& Engine::pool(size_t bytes) {
   return *it->second;
 }
 
-cplx* Engine::mat(int n) { return (cplx*)pool((size_t)n * n * 16).get(stream_); }
-cplx* Engine::vec(int n) { return (cplx*)pool((size_t)((n + 15) / 16) * 256).get(stream_); }
+// A block of a size class; when the device has no room for a new chunk, the
+// chunks of every size class of this engine that hold no handed-out block
+// are freed (memory kept by one workload's pools is then available to the
+// next) and the allocation is tried once more.
+void* Engine::take(size_t bytes) {
+  BlockPool& p = pool(bytes);
+  void* b = p.get(stream_);
+  if (b) return b;
+  if (trim_idle()) b = p.get(stream_);
+  if (!b) throw StatusError(ST_ENOMEM, "device memory exhausted");
+  return b;
+}
+size_t Engine::trim_idle() {
+  size_t rel = 0;
+  for (auto& kv : pools_) rel += kv.second->release_free(stream_);
+  return rel;
+}
+cplx* Engine::mat(int n) { return (cplx*)take((size_t)n * n * 16); }
+cplx* Engine::vec(int n) { return (cplx*)take((size_t)((n + 15) / 16) * 256); }
 void Engine::free_mat(cplx* p, int n) {
   if (p) pool((size_t)n * n * 16).put(p);
 }
@@ -336,7 +369,7 @@ static size_t byte_class(size_t b) {
   size_t c = (b + unit - 1) / unit * unit;
   return (c + 255) / 256 * 256;
 }
-void* Engine::bytes(size_t b) { return pool(byte_class(b)).get(stream_); }
+void* Engine::bytes(size_t b) { return take(byte_class(b)); }
 void Engine::free_bytes(void* p, size_t b) {
   if (p) pool(byte_class(b)).put(p);
 }
@@ -365,12 +398,17 @@ void* Engine::stage(const void* data, size_t nbytes) {
 
 void* Engine::workspace(size_t nbytes) {
   if (nbytes > ws_cap_) {
-    // stream order: the kernels queued before still use the old workspace
+    sync();
     AllocTimer at;
-    if (ws_) VRC_CUDA_CHECK(cudaFreeAsync(ws_, stream_));
+    if (ws_) cudaFree(ws_);
     ws_ = nullptr;
     size_t cap = nbytes + nbytes / 4;
-    if (cudaMallocAsync(&ws_, cap, stream_) != cudaSuccess) {
+    cudaError_t e = cudaMalloc(&ws_, cap);
+    if (e != cudaSuccess) {  // free the pools' idle chunks and try once more
+      (void)cudaGetLastError();
+      e = trim_idle() ? cudaMalloc(&ws_, cap) : e;
+    }
+    if (e != cudaSuccess) {
       (void)cudaGetLastError();
       ws_cap_ = 0;
       throw StatusError(ST_ENOMEM, "workspace allocation failed");
@@ -683,6 +721,40 @@ Engine::CellDev* Engine::prepare_cell(const CellSpec& c) {
     cd->eps_dev = (cplx*)bytes(cd->eps_count * 16);
     VRC_CUDA_CHECK(cudaMemcpyAsync(cd->eps_dev, c.eps.data(), cd->eps_count * 16, cudaMemcpyHostToDevice, stream_));
   }
+  if (c.kind == GEOM_GRID && !c.geom_cb && !std::getenv("VRC_HOST_GEOMETRY") &&
+      (!c.xrules.empty() || !c.yrules.empty())) {
+    // rule tables for the device geometry: bases, then per rule its knots,
+    // values and (spline) second derivatives M = D vals
+    std::vector<double> gd(c.x.begin(), c.x.end());
+    gd.insert(gd.end(), c.y.begin(), c.y.end());
+    std::vector<int> gi;
+    size_t off = 0;
+    for (int axis = 0; axis < 2; ++axis)
+      for (const PwlRule& r : axis == 0 ? c.xrules : c.yrules) {
+        const size_t K = r.zs.size();
+        if (r.index < 0 || r.index >= (int)(axis == 0 ? c.x.size() : c.y.size()) || K < 1 || r.vals.size() != K)
+          throw StatusError(ST_EINVAL, "coordinate rule out of range");
+        const int spline = (r.interp == 1 && !r.D.empty()) ? 1 : 0;
+        gi.insert(gi.end(), {axis, r.index, (int)K, (int)off, spline});
+        gd.insert(gd.end(), r.zs.begin(), r.zs.end());
+        gd.insert(gd.end(), r.vals.begin(), r.vals.end());
+        for (size_t i = 0; i < K; ++i) {
+          double mi = 0.0;
+          if (spline)
+            for (size_t k = 0; k < K; ++k) mi += r.D[i * K + k] * r.vals[k];
+          gd.push_back(mi);
+        }
+        off += 3 * K;
+      }
+    cd->dev_geom = true;
+    cd->nrules = (int)(gi.size() / 5);
+    cd->geo_nd = gd.size();
+    cd->geo_ni = gi.size();
+    cd->geo_d = (double*)bytes(gd.size() * sizeof(double));
+    cd->geo_i = (int*)bytes(std::max<size_t>(1, gi.size()) * sizeof(int));
+    VRC_CUDA_CHECK(cudaMemcpyAsync(cd->geo_d, gd.data(), gd.size() * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    VRC_CUDA_CHECK(cudaMemcpyAsync(cd->geo_i, gi.data(), gi.size() * sizeof(int), cudaMemcpyHostToDevice, stream_));
+  }
   sync();
   return cd;
 }
@@ -698,6 +770,8 @@ void Engine::release_cell(CellDev* cd) {
   free_mat(cd->KyKy, cd->m);
   free_mat(cd->KyKx, cd->m);
   if (cd->eps_dev) free_bytes(cd->eps_dev, cd->eps_count * 16);
+  if (cd->geo_d) free_bytes(cd->geo_d, cd->geo_nd * sizeof(double));
+  if (cd->geo_i) free_bytes(cd->geo_i, std::max<size_t>(1, cd->geo_ni) * sizeof(int));
   delete cd;
 }
 
@@ -706,9 +780,10 @@ void Engine::release_cell(CellDev* cd) {
 // ---------------------------------------------------------------------------
 namespace {
 struct AsmKey {
-  int nx, ny, ncx, ncy, pml, pillar;
+  int nx, ny, ncx, ncy, pml, pillar, devgeom;
   bool operator<(const AsmKey& o) const {
-    return std::tie(nx, ny, ncx, ncy, pml, pillar) < std::tie(o.nx, o.ny, o.ncx, o.ncy, o.pml, o.pillar);
+    return std::tie(nx, ny, ncx, ncy, pml, pillar, devgeom) <
+           std::tie(o.nx, o.ny, o.ncx, o.ncy, o.pml, o.pillar, o.devgeom);
   }
 };
 }  // namespace
@@ -793,6 +868,9 @@ void Engine::assemble_grid(std::vector<SampleReq>& reqs, std::vector<int>* statu
     k.nx = r.spec->nx;
     k.ny = r.spec->ny;
     k.pml = r.spec->pml ? 1 : 0;
+    // a perturbed copy (the geometric adjoint's, with a host callback) shares
+    // its structure's CellDev but not its rules: it stays on the host path
+    k.devgeom = (!r.homogeneous && r.cd && r.cd->dev_geom && r.spec->kind == GEOM_GRID && !r.spec->geom_cb) ? 1 : 0;
     if (r.homogeneous) {
       k.ncx = 2;
       k.ncy = 2;
@@ -817,7 +895,7 @@ void Engine::assemble_grid(std::vector<SampleReq>& reqs, std::vector<int>* statu
     const int nc = ncx - 1, nr = ncy - 1, P = 2 * nx - 1, Q = 2 * ny - 1, m = nx * ny;
     // per-sample workspace (complex elements)
     const size_t o_eps = 0;
-    const size_t o_inv = o_eps + (k.pillar ? (size_t)nr * nc : 0);
+    const size_t o_inv = o_eps + ((k.pillar || k.devgeom) ? (size_t)nr * nc : 0);
     const size_t o_ex = o_inv + (size_t)nr * nc;
     const size_t o_exs = o_ex + (size_t)P * nc;
     const size_t o_ey = o_exs + (size_t)P * nc;
@@ -849,6 +927,7 @@ void Engine::assemble_grid(std::vector<SampleReq>& reqs, std::vector<int>* statu
       std::vector<cplx> homog_eps(B);
       std::vector<std::vector<cplx>> refilled;  // keep alive until sync
       std::vector<double> xv, yv;
+      std::vector<GridGeomJob> gjobs;  // samples whose geometry the device forms
       for (size_t b = 0; b < B; ++b) {
         const SampleReq& r = reqs[idx[c0 + b]];
         const CellSpec& s = *r.spec;
@@ -868,6 +947,9 @@ void Engine::assemble_grid(std::vector<SampleReq>& reqs, std::vector<int>* statu
           xso[1] = xo[1];
           homog_eps[b] = r.eps_h;
           epsp[b] = nullptr;  // set after upload
+        } else if (k.devgeom) {
+          gjobs.push_back({r.z, r.cd->geo_d, r.cd->geo_i, r.cd->nrules, (int)b, r.cd->eps_dev, base + o_eps, nullptr});
+          epsp[b] = nullptr;  // set on the device
         } else {
           s.geometry(r.z, xv, yv);
           std::memcpy(xo, xv.data(), ncx * sizeof(double));
@@ -916,6 +998,9 @@ void Engine::assemble_grid(std::vector<SampleReq>& reqs, std::vector<int>* statu
         const SampleReq& r = reqs[idx[c0 + b]];
         if (r.homogeneous) epsp[b] = upload(&homog_eps[b], 1);
       }
+      for (auto& j : gjobs) j.coords = dcoords + (size_t)j.slot * (2 * ncx + ncy);
+      // one device array of eps pointers: the host's, completed on the device
+      const cplx** d_eps = (const cplx**)upload(epsp);
       auto ptrs = [&](size_t off) {
         std::vector<cplx*> v(B);
         for (size_t b = 0; b < B; ++b) v[b] = ws + b * per + off;
@@ -927,7 +1012,9 @@ void Engine::assemble_grid(std::vector<SampleReq>& reqs, std::vector<int>* statu
           8.0 * B * ((double)P * nr * nc * 2 + (double)Q * nc * nr + (double)P * Q * nr + (double)nx * nx * Q * nr +
                      (double)P * ny * ny * nc + (double)nr * nx * nx * nx + (double)nc * ny * ny * ny);
       const double asm_bytes = 16.0 * B * ((double)nr * nc + 3.0 * m * m);
-      std::unique_ptr<Prof> asm_prof(new Prof(*this, "assembly", asm_flops, asm_bytes, 12 + (k.pillar ? 1 : 0)));
+      std::unique_ptr<Prof> asm_prof(
+          new Prof(*this, "assembly", asm_flops, asm_bytes, 12 + (k.pillar ? 1 : 0) + (gjobs.empty() ? 0 : 1)));
+      if (!gjobs.empty()) grid_geometry(upload(gjobs), (int)gjobs.size(), ncx, ncy, d_eps, stream_);
       if (k.pillar) {
         const CellSpec& s0 = *reqs[idx[c0]].spec;
         double* drad = upload(radius);
@@ -948,16 +1035,14 @@ void Engine::assemble_grid(std::vector<SampleReq>& reqs, std::vector<int>* statu
       twiddles(upload(xp), upload(ex), (int)B, ncx, P, stream_);
       twiddles(upload(xsp), upload(exs), (int)B, ncx, P, stream_);
       twiddles(upload(yp), upload(ey), (int)B, ncy, Q, stream_);
-      std::vector<cplx*> epsmut(B);
-      for (size_t b = 0; b < B; ++b) epsmut[b] = const_cast<cplx*>(epsp[b]);
       std::vector<cplx*> invv(B);
       for (size_t b = 0; b < B; ++b) invv[b] = const_cast<cplx*>(invp[b]);
-      reciprocal(upload(epsmut), upload(invv), (int)B, nr * nc, stream_);
+      reciprocal(const_cast<cplx* const*>(d_eps), upload(invv), (int)B, nr * nc, stream_);
       auto cst = [](const std::vector<cplx*>& v) { return std::vector<const cplx*>(v.begin(), v.end()); };
       auto ax = ptrs(o_ax), bx = ptrs(o_bx), ay = ptrs(o_ay), f2 = ptrs(o_f2);
       // AX = Ex * inv_cm (nc x nr), BX = Ex * eps_cm
       small_gemm(P, nr, nc, upload(cst(ex)), P, upload(cst(invv)), nc, 0, upload(ax), P, (int)B, stream_);
-      small_gemm(P, nr, nc, upload(cst(ex)), P, upload(epsp), nc, 0, upload(bx), P, (int)B, stream_);
+      small_gemm(P, nr, nc, upload(cst(ex)), P, d_eps, nc, 0, upload(bx), P, (int)B, stream_);
       // AY = Ey * inv_cm^T  (Q x nc)
       small_gemm(Q, nc, nr, upload(cst(ey)), Q, upload(cst(invv)), nc, 1, upload(ay), Q, (int)B, stream_);
       // F2 = BX * Ey^T (P x Q)

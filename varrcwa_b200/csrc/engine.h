@@ -107,8 +107,13 @@ class BlockPool {
  public:
   explicit BlockPool(size_t bytes) : bytes_(bytes) {}
   ~BlockPool();
-  void* get(cudaStream_t st);  // a new chunk is allocated in stream order on st
+  // a block (a new 64 MB chunk when none is free); nullptr when the device
+  // has no room for a chunk
+  void* get(cudaStream_t st);
   void put(void* p) { free_.push_back(p); }
+  // frees the chunks none of whose blocks is handed out (cudaFree, which
+  // waits for the device); returns the bytes released
+  size_t release_free(cudaStream_t st);
   size_t bytes() const { return bytes_; }
   size_t blocks() const { return blocks_; }       // blocks created
   size_t free_blocks() const { return free_.size(); }
@@ -117,7 +122,7 @@ class BlockPool {
   size_t bytes_;
   size_t blocks_ = 0;
   std::vector<void*> free_;
-  std::vector<void*> chunks_;
+  std::vector<std::pair<void*, size_t>> chunks_;  // base, blocks
 };
 
 class Engine {
@@ -133,6 +138,8 @@ class Engine {
   void sync();
 
   // memory
+  void* take(size_t bytes);  // a block of a size class (frees idle chunks when the device is full)
+  size_t trim_idle();        // frees every pool chunk with no block handed out
   cplx* mat(int n);
   cplx* vec(int n);
   void free_mat(cplx* p, int n);
@@ -177,6 +184,13 @@ class Engine {
     cplx *Kx = nullptr, *Ky = nullptr, *KxKy = nullptr, *KxKx = nullptr, *KyKy = nullptr, *KyKx = nullptr;
     cplx* eps_dev = nullptr;  // fixed permittivity table (grid / pixels)
     size_t eps_count = 0;
+    // grid cells whose moving coordinates follow tabulated rules: the rule
+    // tables on the device (geometry per sample by grid_geometry)
+    bool dev_geom = false;
+    int nrules = 0;
+    double* geo_d = nullptr;
+    int* geo_i = nullptr;
+    size_t geo_nd = 0, geo_ni = 0;
   };
   CellDev* prepare_cell(const CellSpec& c);
   void release_cell(CellDev* cd);

@@ -75,6 +75,17 @@ void vecnorm_batched(cplx* const* d_X, int batch, int n, cudaStream_t st);
 // ---- assembly -------------------------------------------------------------------
 void pillar_raster(const double* d_radius, cplx* const* d_eps, int batch, int npx, int npy, double Lx,
                    double Ly, cplx eps_in, cplx eps_out, cudaStream_t st);
+// per-sample grid geometry from a structure's rule tables (one job each)
+struct GridGeomJob {
+  double z;
+  const double* gd;  // base x, base y, rule knots / values / second derivatives
+  const int* gi;     // per rule: axis, index, knot count, offset into gd after the bases, spline
+  int nrules, slot;  // slot: entry of the eps pointer array this sample sets
+  const cplx* eps;   // the structure's eps table (ncy-1) x (ncx-1)
+  cplx* refill;      // room for a refilled copy
+  double* coords;    // out: x, sorted x, y
+};
+void grid_geometry(const GridGeomJob* d_jobs, int njobs, int ncx, int ncy, const cplx** d_eps_out, cudaStream_t st);
 void twiddles(const double* const* d_coords, cplx* const* d_out, int batch, int ncoord, int P, cudaStream_t st);
 void reciprocal(cplx* const* d_in, cplx* const* d_out, int batch, int total, cudaStream_t st);
 void small_gemm(int M, int N, int K, const cplx* const* d_A, int lda, const cplx* const* d_B, int ldb, int transB,
