@@ -496,7 +496,7 @@ def run_ours(a, rank, world, local_rank):
             subs["c2"] = measure_forward(ctx, "c2", a.pe, batch=64, steps=3)
         if a.workload != "c4":
             subs["fwd_adjoint"] = measure_fwd_adjoint(ctx, 9, batch=128, steps=10, plain=32)
-            subs["fwd_adjoint_15x15"] = measure_fwd_adjoint(ctx, 15, batch=32, steps=10, plain=32)
+            subs["fwd_adjoint_15x15"] = measure_fwd_adjoint(ctx, 15, batch=64, steps=10, plain=32)
         if not a.no_c5:
             # n = 882 needs large blocks: a fresh context (the pools of the
             # lines above hold their device memory until the context closes)

@@ -444,111 +444,6 @@ __device__ bool small_schur_warp(cplx* T, cplx* U, int nw, int lane, double smln
   return true;
 }
 
-// The same Schur form with every sweep's values carried in registers: lane
-// j owns column j for the row transforms (its entry of the row being
-// reduced) and row j for the column transforms (its entry of the column
-// being reduced), so a rotation's inputs come from the lane's own registers
-// or from one shuffle, and shared memory is written once per entry and
-// read only off the bulge's critical path.  The same operations in the same
-// order per entry as small_schur_warp.
-__device__ bool small_schur_warp_reg(cplx* T, cplx* U, int nw, int lane, double smlnum) {
-  auto t = [&](int r, int c) -> cplx& { return T[c * ALD + r]; };
-  auto u = [&](int r, int c) -> cplx& { return U[c * ALD + r]; };
-  auto shfl = [&](cplx v, int src) {
-    return mk(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
-  };
-  const int itmax = 30 * max(10, nw);
-  int hi = nw - 1, its = 0;
-  while (hi > 0) {
-    __syncwarp();
-    const bool negl = lane + 1 <= hi && small_negligible(T, nw, lane + 1, smlnum);
-    const unsigned bal = __ballot_sync(0xffffffffu, negl);
-    const int lo = bal ? 32 - __clz(bal) : 0;
-    if (lo > 0 && lane == 0) t(lo, lo - 1) = mk(0.0, 0.0);
-    __syncwarp();
-    if (lo == hi) {
-      --hi;
-      its = 0;
-      continue;
-    }
-    if (++its > itmax) return false;
-    const cplx sh = single_shift(T, ALD, lo, hi, its);
-    // carried: cv = T[k][lane] (row being reduced), rv = T[lane][k] (column
-    // being reduced), uv = U[lane][k], lout = T[lane][k-1] of the bulge rows
-    cplx cv = (lane >= lo && lane < nw) ? t(lo, lane) : mk(0.0, 0.0);
-    cplx rv = (lane <= min(lo + 2, hi)) ? t(lane, lo) : mk(0.0, 0.0);
-    cplx uv = lane < nw ? u(lane, lo) : mk(0.0, 0.0);
-    cplx lout = mk(0.0, 0.0);
-    for (int k = lo; k < hi; ++k) {
-      cplx x, y;
-      if (k == lo) {
-        x = csub(shfl(rv, lo), sh);
-        y = shfl(rv, lo + 1);
-      } else {
-        x = shfl(lout, k);
-        y = shfl(lout, k + 1);
-      }
-      cplx beta, tau, v2;
-      refl2(x, y, &beta, &tau, &v2);
-      if (k > lo) {  // the bulge column: beta and an exact zero
-        if (lane == k) t(k, k - 1) = beta;
-        if (lane == k + 1) t(k + 1, k - 1) = mk(0.0, 0.0);
-      }
-      // row transform of rows k, k+1 (lane = column j >= k)
-      const cplx bk = shfl(rv, k + 1);  // T[k+1][k] after the previous column transform
-      cplx ra = mk(0.0, 0.0), rb = mk(0.0, 0.0);
-      if (lane >= k && lane < nw) {
-        ra = lane == k ? rv : cv;
-        rb = lane == k ? bk : t(k + 1, lane);
-        rotate2<true>(ra, rb, tau, v2);
-        if (lane >= k + 2) t(k, lane) = ra;  // row k is done with row transforms
-        cv = rb;                             // T[k+1][lane], the next row's entry
-      }
-      // column transform of columns k, k+1 (lane = row r <= min(k+2, hi))
-      const cplx up = shfl(ra, k + 1);  // T[k][k+1] after the row transform
-      const cplx dn = shfl(ra, k);      // unused by most lanes
-      const cplx lw = shfl(rb, k);      // T[k+1][k] after the row transform
-      (void)dn;
-      __syncwarp();  // row k's stores are visible to the column transforms below
-      const int re = min(k + 2, hi);
-      if (lane <= re) {
-        cplx p, w;
-        if (lane < k) {
-          p = rv;
-          w = t(lane, k + 1);
-        } else if (lane == k) {
-          p = ra;
-          w = up;
-        } else if (lane == k + 1) {
-          p = lw;
-          w = rb;
-        } else {  // k + 2: below the Hessenberg band in column k
-          p = mk(0.0, 0.0);
-          w = t(k + 2, k + 1);
-        }
-        rotate2<false>(p, w, tau, v2);
-        if (lane <= k) t(lane, k) = p;  // column k is done
-        else lout = p;                  // the next bulge (rows k+1, k+2)
-        rv = w;                         // T[lane][k+1]
-        if (lane == k + 1) cv = w;      // the next row transform's diagonal entry
-      }
-      if (lane < nw) {
-        cplx p = uv, w = u(lane, k + 1);
-        rotate2<false>(p, w, tau, v2);
-        u(lane, k) = p;
-        uv = w;
-      }
-    }
-    // the last rotation's carried entries
-    if (lane >= hi + 1 && lane < nw) t(hi, lane) = cv;
-    if (lane <= hi) t(lane, hi) = rv;
-    if (lane == hi) t(hi, hi - 1) = lout;
-    if (lane < nw) u(lane, hi) = uv;
-  }
-  __syncwarp();
-  return true;
-}
-
 // Swaps the adjacent diagonal entries k, k+1 of the upper triangular T and
 // updates U (LAPACK xTREXC's step: T <- G T G^H, U <- U G^H).  One warp.
 __device__ void schur_swap_warp(cplx* T, cplx* U, int nw, int k, int lane) {
@@ -681,7 +576,7 @@ __device__ int aed_deflate_warp(cplx* T, cplx* U, cplx* v, cplx* ev, int nw, cpl
 template <int MINB>
 __global__ void __launch_bounds__(QR_THREADS, MINB)
     hqr_kernel(cplx* const* __restrict__ Hs, void* const* __restrict__ logs, cplx* const* __restrict__ Ws, int n,
-               int sweep_cap, long long rot_cap, int* __restrict__ status, int aed_min, int aed_w, int wreg) {
+               int sweep_cap, long long rot_cap, int* __restrict__ status, int aed_min, int aed_w) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx* D = reinterpret_cast<cplx*>(smem_raw);  // [QD][QLD] column-major window
   cplx* s_tau = D + QD * QLD;                   // [NBMAX][QB]
@@ -789,8 +684,7 @@ __global__ void __launch_bounds__(QR_THREADS, MINB)
         if (warp == 0) {
           int ns = -1;
           const long long c0 = clock64();
-          const bool conv =
-              wreg ? small_schur_warp_reg(T, U, jw, lane, smlnum) : small_schur_warp(T, U, jw, lane, smlnum);
+          const bool conv = small_schur_warp(T, U, jw, lane, smlnum);
           const long long c1 = clock64();
           if (conv) ns = aed_deflate_warp(T, U, s_aedv, s_aedev, jw, s0, lane, smlnum);
           if (lane == 0) {
@@ -1209,11 +1103,6 @@ void schur_batched(cplx* const* d_H, cplx* const* d_Z, cplx* const* d_W, void* c
     return e ? std::max(0, std::atoi(e)) : -1;
   }();
   const int aed_min = aed_env >= 0 ? aed_env : (n <= 128 ? 0 : aed_w);
-  // the window's Schur form with register-carried sweeps (VRC_QR_WREG=1)
-  static const int wreg = [] {
-    const char* e = std::getenv("VRC_QR_WREG");
-    return e ? std::atoi(e) : 0;
-  }();
   ensure_smem((const void*)hqr, QR_SMEM);
   ensure_smem((const void*)qr_replay_rows_kernel, RP_SMEM);
   ensure_smem((const void*)qr_replay_cols_kernel, RP_SMEM);
@@ -1225,7 +1114,7 @@ void schur_batched(cplx* const* d_H, cplx* const* d_Z, cplx* const* d_W, void* c
     const int nb = min(65535, batch - b0);
     if (parts & SCHUR_ITERATE)
       hqr<<<nb, QR_THREADS, QR_SMEM, st>>>(d_H + b0, d_logs + b0, d_W + b0, n, cc, rc,
-                                                  d_status ? d_status + b0 : nullptr, aed_min, aed_w, wreg);
+                                                  d_status ? d_status + b0 : nullptr, aed_min, aed_w);
     if (parts & SCHUR_REPLAY) {
       qr_replay_rows_kernel<<<dim3(2 * row_blocks, nb), RP_THREADS, rp_smem, st>>>(d_H + b0, d_Z + b0, d_logs + b0,
                                                                                   n, cc, row_blocks);
